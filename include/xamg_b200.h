@@ -1,0 +1,152 @@
+/*
+ * Extension entry points of the B200 solve-phase library (libxamg_c_api.so).
+ *
+ * These stand beside the reference C API of xamg_c_api.h. They expose the
+ * device kernels one by one (device pointers in, for kernel-level parity
+ * tests and benchmarks), the setup results a caller may want to inspect
+ * (narrowed index arrays, hierarchy, statistics), and the matrix generators
+ * of the benchmark configurations. Each entry names the reference function
+ * whose behaviour it carries, or says that it has no counterpart.
+ */
+#ifndef XAMG_B200_H_
+#define XAMG_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. The reference returns 0 from every call and asserts on
+ * errors (api/c/xamg_c_api.cpp:170-597); here errors come back as these. */
+#define XAMG_OK 0
+#define XAMG_ERR_INVALID_HANDLE (-1)
+#define XAMG_ERR_INVALID_ARG (-2)
+#define XAMG_ERR_NV_MISMATCH (-3)
+#define XAMG_ERR_CUDA (-4)
+#define XAMG_ERR_BREAKDOWN (-5)
+#define XAMG_ERR_TIMEOUT (-6)
+#define XAMG_ERR_NOT_INITIALIZED (-7)
+#define XAMG_ERR_UNSUPPORTED (-8)
+#define XAMG_ERR_ALLOC (-9)
+#define XAMG_ERR_INTERNAL (-10)
+
+/* Message of the last failed call (no counterpart in the reference). */
+int XAMG_b200_last_error(char *buf, size_t len);
+
+/* Build information: returns the number of kernels compiled in and writes
+ * the target architecture string (no counterpart in the reference). */
+int XAMG_b200_build_info(char *buf, size_t len);
+
+/* A CSR block resident in device memory, with XAMG's narrowed column type
+ * (col_bytes = 1, 2 or 4; csr_matrix.h:47-86 with I2 in {u8,u16,u32}).
+ * Row pointers are 32-bit. Values are double (val_f32 = 0) or float. */
+typedef struct {
+    uint64_t nrows, ncols, nnz;
+    const uint32_t *row;
+    const void *col;
+    const void *val;
+    int col_bytes;
+    int val_f32;
+} XAMG_b200_csr;
+
+/* y = A x (mode 0, blas2::Ax_y, src/blas2/detail/csr_matvec.inl:148-260) or
+ * y += A x (mode 1, blas2::Axpy, csr_matvec.inl:32-144). x and y are device
+ * arrays [rows][nv] (element (i,k) at i*nv+k) of the matrix value type.
+ * Each (row, k) is accumulated sequentially over the row's entries with
+ * separately rounded multiply and add, as the reference does. */
+int XAMG_b200_spmv(const XAMG_b200_csr *A, const void *x, void *y, int nv, int mode,
+                   void *stream);
+
+/* v = A x and dot[k] = (v, z)_k in one pass (the blas2::Ax_y + blas::dot pair
+ * of merged_pbicgstab.inl:140-153). Double only; dot_out is a host array of
+ * nv values; the call synchronises the stream. */
+int XAMG_b200_spmv_dot(const XAMG_b200_csr *A, const double *x, double *v, const double *z,
+                       double *dot_out, int nv, void *stream);
+
+/* dot[k] = (x, y)_k over n rows (blas::dot, src/blas/detail/blas.inl:463-532)
+ * in the library's fixed reduction order. Host output; synchronises. */
+int XAMG_b200_dot(uint64_t n, int nv, const double *x, const double *y, double *dot_out,
+                  void *stream);
+
+/* merged_bicgstab_group1/2/4 (blas_merged_bicgstab.inl:32-194) on device
+ * arrays; the reductions come back in host arrays of nv values. */
+int XAMG_b200_group1(uint64_t n, int nv, double *r0, const double *b, double *p, double *r,
+                     double *rho0_out, void *stream);
+int XAMG_b200_group2(uint64_t n, int nv, const double *t, const double *s, double *phi_out,
+                     double *psi_out, double *theta_out, void *stream);
+int XAMG_b200_group4(uint64_t n, int nv, const double *s, const double *t, const double *r0,
+                     double *r, const double *omega_host, double *rho_out, void *stream);
+
+/* XAMG's index narrowing (bit_operations.h:119-129, csr_matrix.h:455-461). */
+uint16_t XAMG_b200_define_int_type(uint64_t range);
+uint16_t XAMG_b200_encode_hash(uint64_t nnz, uint64_t ncols, uint64_t block_nrows,
+                               uint64_t block_ncols, int f32, int reduced_prec);
+
+/* Matrix generators of the benchmark configurations (host arrays; return
+ * the number of nonzeros, or a negative status). The arrays must hold
+ * nx*ny*nz+1 row pointers and 7 (or 27) entries per row.
+ *  - cube: the reference's 7-point Laplacian, examples/common/generator/cube.inl:28-174.
+ *  - diffusion: variable-coefficient diffusion with per-cell coefficient
+ *    kappa = exp(sigma * N(0,1)) from `seed`, 7-point finite volumes with
+ *    harmonic face averages (stencil 7) or trilinear Q1 finite elements
+ *    (stencil 27); aniso_z scales the z-direction conductivity. No
+ *    counterpart in the reference. */
+int64_t XAMG_b200_generate_cube(uint64_t nx, uint64_t ny, uint64_t nz, uint32_t *row,
+                                uint32_t *col, double *val);
+int64_t XAMG_b200_generate_diffusion(int stencil, uint64_t nx, uint64_t ny, uint64_t nz,
+                                     double sigma, double aniso_z, uint64_t seed, uint32_t *row,
+                                     uint32_t *col, double *val);
+
+/* Solver introspection (no counterpart in the reference; it keeps the same
+ * data in solver_stats, solver.h:48-66). nv entries per array. */
+int XAMG_b200_solver_stats(size_t sid, int *iters, int *conv, double *abs_res, double *rel_res,
+                           int nv);
+
+/* The multigrid hierarchy a solver built and uploaded: number of levels
+ * (1 when the solver has no multigrid). */
+int XAMG_b200_solver_nlevels(size_t sid);
+
+/* Shape of level matrix `which` (0 = A, 1 = R, 2 = P) as uploaded: sizes,
+ * narrowed column width, value type, XAMG hash, eigenvalue estimates. */
+int XAMG_b200_solver_level_info(size_t sid, int level, int which, uint64_t *nrows,
+                                uint64_t *ncols, uint64_t *nnz, int *col_bytes, int *val_f32,
+                                uint16_t *hash, double *min_eig, double *max_eig);
+
+/* Copy level matrix `which` back from the device exactly as stored: row
+ * pointers (u32), narrowed columns (col_bytes each), values (float/double). */
+int XAMG_b200_solver_level_download(size_t sid, int level, int which, uint32_t *row, void *col,
+                                    void *val);
+
+/* The double-precision hierarchy the host setup built, before narrowing and
+ * precision conversion (the equivalent of what hypre hands to XAMG in
+ * hypre_base.inl:337-403): which = 0 A_l, 2 P_l. */
+int XAMG_b200_solver_hierarchy_export(size_t sid, int level, int which, uint32_t *row,
+                                      uint32_t *col, double *val);
+
+/* Device pointers of an uploaded level matrix (which = 0 A, 1 R, 2 P), for
+ * running the kernel entry points on the solver's own data (no counterpart). */
+int XAMG_b200_solver_level_csr(size_t sid, int level, int which, XAMG_b200_csr *out);
+
+/* Number of kernels this library has launched since it was loaded (no
+ * counterpart; used to account for the device work of a timed region). */
+uint64_t XAMG_b200_kernel_launches(void);
+
+/* The CUDA stream every library call is ordered on (a cudaStream_t), for
+ * callers that time or order their own work against it (no counterpart). */
+void *XAMG_b200_stream(void);
+
+/* Select the CUDA device the library will use; must precede XAMG_init and
+ * the first call that touches the GPU (no counterpart: the reference binds
+ * ranks to cores through XAMG_NUMACONF instead). */
+int XAMG_b200_set_device(int device);
+
+/* Device address of a vector's [size][nv] storage (no counterpart). */
+int XAMG_b200_vector_device_ptr(size_t vid, void **ptr);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* XAMG_B200_H_ */

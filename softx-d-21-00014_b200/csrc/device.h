@@ -1,0 +1,137 @@
+// Device-side containers of the library: owned device buffers, the per-process
+// context (stream, reduction scratch, pinned staging), device vectors with
+// XAMG's zero/initialised flags, and narrowed device CSR blocks.
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "common.h"
+#include "hcsr.h"
+#include "kernels.cuh"
+
+namespace xg {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    explicit DevBuf(size_t b) { alloc(b); }
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    DevBuf(DevBuf &&o) noexcept : p(o.p), bytes(o.bytes) {
+        o.p = nullptr;
+        o.bytes = 0;
+    }
+    DevBuf &operator=(DevBuf &&o) noexcept {
+        if (this != &o) {
+            release();
+            p = o.p;
+            bytes = o.bytes;
+            o.p = nullptr;
+            o.bytes = 0;
+        }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+    void alloc(size_t b) {
+        release();
+        if (b) {
+            cudaError_t e = cudaMalloc(&p, b);
+            if (e != cudaSuccess) {
+                p = nullptr;
+                throw Error(XAMG_ERR_ALLOC, std::string("cudaMalloc(") + std::to_string(b) +
+                                                " bytes): " + cudaGetErrorString(e));
+            }
+        }
+        bytes = b;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <typename T>
+    T *as() const {
+        return (T *)p;
+    }
+};
+
+// Process-wide state created by XAMG_init (or lazily by the first call that
+// needs the GPU).
+struct Ctx {
+    cudaStream_t stream = nullptr;
+    DevBuf red_part;    // canonical-reduction partials: BMAX x 32 x 3 doubles
+    DevBuf red_ticket;  // one counter, zero between launches
+    DevBuf red_out;     // 96 doubles for reductions returned to the host
+    double *pinned = nullptr;  // 256 doubles of pinned host memory
+    int device = 0;
+    int device_request = -1;  // set by XAMG_b200_set_device before init
+    bool ready = false;
+
+    void init();
+    void shutdown();
+    k::RedArgs red() const { return k::RedArgs{red_part.p, red_ticket.as<unsigned>()}; }
+};
+
+Ctx &ctx();
+Ctx &ctx_uninit();  // the context object without initialising it
+
+// Count of kernel launches issued by this library (all launch helpers bump it).
+extern uint64_t g_kernel_launches;
+
+// A device vector: size rows of nv interleaved values (float or double), plus
+// XAMG's state flags (vector.h:90-99). `zero` means "the contents are known to
+// be zero and need not be read"; `init` means "has been written".
+struct DVec {
+    uint64_t n = 0;
+    int nv = 0;
+    bool f32 = false;
+    bool zero = true;
+    bool init = false;
+    std::shared_ptr<DevBuf> buf;
+
+    void alloc(uint64_t n_, int nv_, bool f32_) {
+        n = n_;
+        nv = nv_;
+        f32 = f32_;
+        buf = std::make_shared<DevBuf>(n * nv * (f32 ? 4 : 8));
+        zero = true;
+        init = false;
+    }
+    template <typename T>
+    T *p() const {
+        return buf ? (T *)buf->p : nullptr;
+    }
+    uint64_t elems() const { return n * (uint64_t)nv; }
+};
+
+// A CSR block on the device with XAMG's narrowed column type.
+struct DCsr {
+    uint64_t nrows = 0, ncols = 0, nnz = 0;
+    int col_bytes = 4;
+    bool f32 = false;
+    uint16_t hash = 0;
+    DevBuf row, col, val;
+
+    template <typename F>
+    k::CsrArgs<F> args() const {
+        return k::CsrArgs<F>{row.as<uint32_t>(), col.p, val.as<F>(), nrows};
+    }
+    bool empty() const { return nnz == 0; }
+};
+
+// Upload `h` narrowed per XAMG's rule (define_int_type on ncols for the
+// column width; the I1 row-pointer width only enters the hash since row
+// pointers stay 32-bit on the device). reduced_prec stores float values.
+void upload_csr(const HCsr &h, DCsr &d, bool f32, bool narrow, cudaStream_t s);
+void download_csr(const DCsr &d, uint32_t *row, void *col, void *val);
+
+template <typename T>
+void upload(DevBuf &b, const std::vector<T> &v, cudaStream_t s) {
+    b.alloc(v.size() * sizeof(T));
+    if (!v.empty()) XG_CUDA(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T),
+                                            cudaMemcpyHostToDevice, s));
+}
+
+}  // namespace xg

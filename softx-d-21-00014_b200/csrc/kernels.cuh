@@ -1,0 +1,672 @@
+// Device kernels of the solve phase (sm_100a).
+//
+// Layout: every n-vector with nv right-hand sides is stored row-major
+// interleaved, element (i, k) at i*NV + k, as XAMG stores it
+// (src/primitives/vector/vector.h:509-525). CSR blocks keep 32-bit row
+// pointers, XAMG-narrowed column indices (u8/u16/u32) and float or double
+// values.
+//
+// Arithmetic: products and sums use the round-to-nearest intrinsics
+// (__dmul_rn, __dadd_rn, ...), which the compiler never contracts into FMA,
+// and each row is accumulated in the reference's order (entry by entry, from
+// 0 for y = Ax, from y for y += Ax). Every element a kernel writes therefore
+// equals, bit for bit, what the reference's -ffp-contract=off CPU loop
+// computes.
+//
+// Row schedule ("canonical order"): a block has 256 threads; thread t works on
+// row slot t/NV and right-hand side t%NV, so a tile covers 256/NV consecutive
+// rows and consecutive threads read consecutive x entries of a row. Tiles are
+// dealt round-robin to B = min(ntiles, 1184) blocks (8 per SM on 148 SMs).
+// Dot products are accumulated per thread in tile order, combined within a
+// warp by an xor butterfly (offsets 16..NV), across the 8 warps in warp
+// order, and across blocks by the last block to finish: lane l sums blocks
+// l, l+32, ... and a full butterfly finishes. The order depends only on
+// (n, NV), so results are reproducible run to run and the CPU oracle can
+// replay it exactly.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace xg {
+namespace k {
+
+constexpr int CT = 256;     // threads per block
+constexpr int BMAX = 1184;  // block cap of the canonical schedule
+
+// ---------------------------------------------------------------------------
+// Separately rounded arithmetic
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double dvd(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float dvd(float a, float b) { return __fdiv_rn(a, b); }
+
+template <typename T>
+__device__ __forceinline__ T shfl_xor(T v, int off) {
+    return __shfl_xor_sync(0xffffffffu, v, off);
+}
+
+template <typename T>
+__device__ __forceinline__ T ld_cg(const T *p) {
+    return __ldcg(p);
+}
+
+// ---------------------------------------------------------------------------
+// Per-solver scalar block: NV-wide FP64 scalars of the Krylov recurrences,
+// kept in device memory so that no kernel waits on the host for them.
+// ---------------------------------------------------------------------------
+enum Sc : int {
+    SC_RHO = 0,
+    SC_RHO0,
+    SC_RES,
+    SC_ALPHA,
+    SC_OMEGA,
+    SC_BETA,
+    SC_PHI,
+    SC_PSI,
+    SC_THETA,
+    SC_SCAL1,
+    SC_SCAL2,
+    SC_SCAL3,
+    SC_SCAL4,
+    SC_ICONV,
+    SC_ALPHA_C,
+    SC_OMEGA_C,
+    SC_NSCAL,  // -(omega*beta), the v coefficient of the p update
+    SC_RELAX,
+    SC_COUNT
+};
+constexpr int SC_STRIDE = 32;
+
+__host__ __device__ inline int canon_rows_per_tile(int nv) { return CT / nv; }
+
+inline int canon_blocks(uint64_t n, int nv) {
+    const uint64_t R = CT / nv;
+    const uint64_t nt = (n + R - 1) / R;
+    return (int)(nt < (uint64_t)BMAX ? (nt == 0 ? 1 : nt) : (uint64_t)BMAX);
+}
+
+// ---------------------------------------------------------------------------
+// Canonical reduction: block partials, then the last block finishes.
+// ---------------------------------------------------------------------------
+struct RedArgs {
+    void *part;        // [BMAX][32][3] partial sums (element type of the kernel)
+    unsigned *ticket;  // zero between launches
+};
+
+template <typename T, int NV, int NRED, class Fin>
+__device__ __forceinline__ void canon_finish(T (&acc)[NRED], const RedArgs &ra, const Fin &fin) {
+    __shared__ T wsum[8 * NV * NRED];
+    __shared__ T sums[NV * NRED];
+    __shared__ int is_last;
+    T *part = (T *)ra.part;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int r = 0; r < NRED; ++r) {
+        T v = acc[r];
+#pragma unroll
+        for (int off = 16; off >= NV; off >>= 1) v = add(v, shfl_xor(v, off));
+        if (lane < NV) wsum[(warp * NV + lane) * NRED + r] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < NV * NRED) {
+        const int o = threadIdx.x;  // o = k*NRED + r
+        T s = wsum[o];
+#pragma unroll
+        for (int w = 1; w < 8; ++w) s = add(s, wsum[w * NV * NRED + o]);
+        part[(size_t)blockIdx.x * NV * NRED + o] = s;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned t = atomicAdd(ra.ticket, 1u);
+        is_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    for (int o = warp; o < NV * NRED; o += 8) {
+        T a = T(0);
+        for (unsigned bb = lane; bb < gridDim.x; bb += 32)
+            a = add(a, ld_cg(&part[(size_t)bb * NV * NRED + o]));
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) a = add(a, shfl_xor(a, off));
+        if (lane == 0) sums[o] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *ra.ticket = 0u;
+    if (threadIdx.x < NV) fin(threadIdx.x, &sums[threadIdx.x * NRED]);
+}
+
+// ---------------------------------------------------------------------------
+// CSR SpMV with a compile-time epilogue.
+//   acc = epi.init(i,k); for j in row i: acc = acc + x[col[j]*NV+k] * val[j]
+//   epi.store(i, k, acc, terms[NRED])
+// FX is the element type x is stored in; it is converted to F on load (the
+// fused form of vector::convert before a reduced-precision restriction).
+// ---------------------------------------------------------------------------
+template <typename F>
+struct CsrArgs {
+    const uint32_t *row;
+    const void *col;
+    const F *val;
+    uint64_t n;
+};
+
+template <typename F, typename FX, typename I, int NV, int NRED, class Epi>
+__global__ void __launch_bounds__(CT)
+    k_spmv(CsrArgs<F> A, const FX *__restrict__ x, Epi epi, RedArgs ra) {
+    constexpr int R = CT / NV;
+    const int rt = threadIdx.x / NV, k = threadIdx.x % NV;
+    const uint32_t *__restrict__ row = A.row;
+    const I *__restrict__ col = (const I *)A.col;
+    const F *__restrict__ val = A.val;
+    const uint64_t ntiles = (A.n + R - 1) / R;
+    F acc[NRED > 0 ? NRED : 1];
+#pragma unroll
+    for (int r = 0; r < (NRED > 0 ? NRED : 1); ++r) acc[r] = F(0);
+    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const uint64_t i = tile * R + rt;
+        if (i < A.n) {
+            F y = epi.init(i, k);
+            const uint32_t j0 = __ldg(&row[i]), j1 = __ldg(&row[i + 1]);
+            for (uint32_t j = j0; j < j1; ++j) {
+                const uint64_t c = (uint64_t)__ldg(&col[j]);
+                const F xv = (F)__ldg(&x[c * NV + k]);
+                y = add(y, mul(xv, __ldg(&val[j])));
+            }
+            epi.store(i, k, y, acc);
+        }
+    }
+    if constexpr (NRED > 0) canon_finish<F, NV, NRED>(acc, ra, epi);
+}
+
+// Element-wise canonical kernel (same schedule, no matrix).
+template <typename F, int NV, int NRED, class Epi>
+__global__ void __launch_bounds__(CT) k_rows(uint64_t n, Epi epi, RedArgs ra) {
+    constexpr int R = CT / NV;
+    const int rt = threadIdx.x / NV, k = threadIdx.x % NV;
+    const uint64_t ntiles = (n + R - 1) / R;
+    F acc[NRED > 0 ? NRED : 1];
+#pragma unroll
+    for (int r = 0; r < (NRED > 0 ? NRED : 1); ++r) acc[r] = F(0);
+    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const uint64_t i = tile * R + rt;
+        if (i < n) epi.elem(i, k, acc);
+    }
+    if constexpr (NRED > 0) canon_finish<F, NV, NRED>(acc, ra, epi);
+}
+
+// Scalar-only kernel: one thread per right-hand side.
+template <class Op>
+__global__ void k_scalar(int nv, Op op) {
+    if ((int)threadIdx.x < nv) op(threadIdx.x);
+}
+
+// ---------------------------------------------------------------------------
+// Epilogues. `NoFin` is used when the epilogue has no reduction.
+// ---------------------------------------------------------------------------
+struct NoFin {
+    template <typename T>
+    __device__ void operator()(int, const T *) const {}
+};
+
+// y = A x  (csr_matvec.inl:213-231)
+template <typename F, int NV>
+struct EStore : NoFin {
+    F *y;
+    __device__ F init(uint64_t, int) const { return F(0); }
+    template <int NR>
+    __device__ void store(uint64_t i, int k, F v, F (&)[NR]) const { y[i * NV + k] = v; }
+};
+
+// y += A x  (csr_matvec.inl:106-120: accumulate directly into y)
+template <typename F, int NV>
+struct EAxpy : NoFin {
+    F *y;
+    __device__ F init(uint64_t i, int k) const { return y[i * NV + k]; }
+    template <int NR>
+    __device__ void store(uint64_t i, int k, F v, F (&)[NR]) const { y[i * NV + k] = v; }
+};
+
+// r = 1*b + (-1)*(A x)  (solver.h:249-250: Ax_y then axpby(1, b, -1, r)),
+// optionally with (r, r) (vector_norm, blas.inl:537-555).
+template <typename F, int NV, bool NORM>
+struct EResid {
+    F *r;
+    const F *b;
+    double *out;  // NORM: sums land here (nv values)
+    __device__ F init(uint64_t, int) const { return F(0); }
+    template <int NR>
+    __device__ void store(uint64_t i, int k, F v, F (&acc)[NR]) const {
+        const F rv = add(mul(F(1), b[i * NV + k]), mul(F(-1), v));
+        r[i * NV + k] = rv;
+        if constexpr (NORM) acc[0] = add(acc[0], mul(rv, rv));
+    }
+    __device__ void operator()(int k, const F *s) const {
+        if constexpr (NORM) out[k] = (double)s[0];
+    }
+};
+
+// merged_bicgstab_group1 after r0 = A x (blas_merged_bicgstab.inl:60-72):
+// r0 = b - r0; rho0 += r0*r0; p = r = r0. The finaliser also copies
+// rho0 into rho (merged_bicgstab.inl:119).
+template <int NV>
+struct EGroup1 {
+    double *r0, *p, *r;
+    const double *b;
+    double *sc;
+    __device__ double init(uint64_t, int) const { return 0.0; }
+    template <int NR>
+    __device__ void store(uint64_t i, int k, double v, double (&acc)[NR]) const {
+        const uint64_t e = i * NV + k;
+        const double rv = sub(b[e], v);
+        r0[e] = rv;
+        p[e] = rv;
+        r[e] = rv;
+        acc[0] = add(acc[0], mul(rv, rv));
+    }
+    __device__ void operator()(int k, const double *s) const {
+        sc[SC_RHO0 * SC_STRIDE + k] = s[0];
+        sc[SC_RHO * SC_STRIDE + k] = s[0];
+    }
+};
+
+// v = A p_ ; scal1 = (v, r0) ; alpha = rho / scal1
+// (merged_pbicgstab.inl:140-155)
+template <int NV>
+struct EDotAlpha {
+    double *v;
+    const double *r0;
+    double *sc;
+    __device__ double init(uint64_t, int) const { return 0.0; }
+    template <int NR>
+    __device__ void store(uint64_t i, int k, double y, double (&acc)[NR]) const {
+        const uint64_t e = i * NV + k;
+        v[e] = y;
+        acc[0] = add(acc[0], mul(y, r0[e]));
+    }
+    __device__ void operator()(int k, const double *s) const {
+        sc[SC_SCAL1 * SC_STRIDE + k] = s[0];
+        sc[SC_ALPHA * SC_STRIDE + k] = dvd(sc[SC_RHO * SC_STRIDE + k], s[0]);
+    }
+};
+
+// t = A s_ ; phi = (t,s), psi = (t,t), theta = (s,s); omega = phi/psi;
+// res = theta - omega*phi; alpha_c = iconv*alpha; omega_c = iconv*omega
+// (merged_pbicgstab.inl:168-192)
+template <int NV>
+struct EDot3 {
+    double *t;
+    const double *s;
+    double *sc;
+    __device__ double init(uint64_t, int) const { return 0.0; }
+    template <int NR>
+    __device__ void store(uint64_t i, int k, double y, double (&acc)[NR]) const {
+        const uint64_t e = i * NV + k;
+        t[e] = y;
+        const double sv = s[e];
+        acc[0] = add(acc[0], mul(y, sv));
+        acc[1] = add(acc[1], mul(y, y));
+        acc[2] = add(acc[2], mul(sv, sv));
+    }
+    __device__ void operator()(int k, const double *s3) const {
+        double *S = sc;
+        const double phi = s3[0], psi = s3[1], theta = s3[2];
+        S[SC_PHI * SC_STRIDE + k] = phi;
+        S[SC_PSI * SC_STRIDE + k] = psi;
+        S[SC_THETA * SC_STRIDE + k] = theta;
+        const double omega = dvd(phi, psi);
+        S[SC_OMEGA * SC_STRIDE + k] = omega;
+        double res = mul(omega, phi);
+        res = add(mul(1.0, theta), mul(-1.0, res));
+        S[SC_RES * SC_STRIDE + k] = res;
+        const double ic = S[SC_ICONV * SC_STRIDE + k];
+        S[SC_ALPHA_C * SC_STRIDE + k] = mul(ic, S[SC_ALPHA * SC_STRIDE + k]);
+        S[SC_OMEGA_C * SC_STRIDE + k] = mul(ic, omega);
+    }
+};
+
+// One Jacobi sweep with x not zero (blas_merged_jacobi.inl:74-80):
+// x_out = x_in + relax*d*(b - A x_in)
+template <typename F, int NV>
+struct EJacobi : NoFin {
+    F *xout;
+    const F *xin, *b, *d;
+    F relax;
+    __device__ F init(uint64_t, int) const { return F(0); }
+    template <int NR>
+    __device__ void store(uint64_t i, int k, F v, F (&)[NR]) const {
+        const uint64_t e = i * NV + k;
+        xout[e] = add(xin[e], mul(mul(relax, d[i]), sub(b[e], v)));
+    }
+};
+
+// Chebyshev, first polynomial step (chebyshev.inl:179-190):
+// r = b - A x; r := r*isd; t1 = c_top * r; t1 := t1*isd (input of the next
+// SpMV). x_zero: r = 1*b without the SpMV (used by k_rows through elem()).
+template <typename F, int NV>
+struct ECheby0 : NoFin {
+    F *rs, *t1s;
+    const F *b, *isd;
+    F c;
+    __device__ F init(uint64_t, int) const { return F(0); }
+    __device__ void finish(uint64_t i, int k, F r) const {
+        const uint64_t e = i * NV + k;
+        const F d = isd[i];
+        const F rr = mul(r, d);
+        rs[e] = rr;
+        t1s[e] = mul(mul(c, rr), d);
+    }
+    template <int NR>
+    __device__ void store(uint64_t i, int k, F v, F (&)[NR]) const {
+        const uint64_t e = i * NV + k;
+        finish(i, k, add(mul(F(1), b[e]), mul(F(-1), v)));
+    }
+    template <int NR>
+    __device__ void elem(uint64_t i, int k, F (&)[NR]) const {
+        finish(i, k, mul(F(1), b[i * NV + k]));
+    }
+};
+
+// Chebyshev inner step i (chebyshev.inl:189-199):
+// t2 = A t1s; t2 := t2*isd; t1 = c_i*rs + 1*t2; then either t1s_out = t1*isd
+// (more steps) or x = 1*(t1*isd) + 1*x (last step; x_zero: x = 1*(t1*isd)).
+template <typename F, int NV>
+struct ECheby1 : NoFin {
+    F *out;  // next t1s, or x on the last step
+    const F *rs, *isd;
+    F c;
+    int last, x_zero;
+    __device__ F init(uint64_t, int) const { return F(0); }
+    template <int NR>
+    __device__ void store(uint64_t i, int k, F v, F (&)[NR]) const {
+        const uint64_t e = i * NV + k;
+        const F d = isd[i];
+        const F t2 = mul(v, d);
+        const F t1 = add(mul(c, rs[e]), mul(F(1), t2));
+        const F t1d = mul(t1, d);
+        if (!last)
+            out[e] = t1d;
+        else if (x_zero)
+            out[e] = mul(F(1), t1d);
+        else
+            out[e] = add(mul(F(1), t1d), mul(F(1), out[e]));
+    }
+};
+
+// Prolongation with a reduced-precision P (mg.inl:241-249): the product is
+// accumulated in float, converted to double, then x = 1*t + 1*x
+// (x_zero: x = 1*t, the ax_y branch of axpby).
+template <int NV>
+struct EProlongMixed : NoFin {
+    double *x;
+    int x_zero;
+    __device__ float init(uint64_t, int) const { return 0.0f; }
+    template <int NR>
+    __device__ void store(uint64_t i, int k, float v, float (&)[NR]) const {
+        const uint64_t e = i * NV + k;
+        const double t = (double)v;
+        x[e] = x_zero ? mul(1.0, t) : add(mul(1.0, t), mul(1.0, x[e]));
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Element-wise epilogues for k_rows
+// ---------------------------------------------------------------------------
+
+// dot[k] = (x, y)_k  (blas.inl:504-519)
+template <typename F, int NV>
+struct EDot {
+    const F *x, *y;
+    double *out;
+    template <int NR>
+    __device__ void elem(uint64_t i, int k, F (&acc)[NR]) const {
+        const uint64_t e = i * NV + k;
+        acc[0] = add(acc[0], mul(x[e], y[e]));
+    }
+    __device__ void operator()(int k, const F *s) const { out[k] = (double)s[0]; }
+};
+
+// merged_bicgstab_group2 (blas_merged_bicgstab.inl:127-134)
+template <int NV>
+struct EGroup2 {
+    const double *t, *s;
+    double *out;  // phi, psi, theta at out[0..nv), out[32..), out[64..)
+    template <int NR>
+    __device__ void elem(uint64_t i, int k, double (&acc)[NR]) const {
+        const uint64_t e = i * NV + k;
+        const double tv = t[e], sv = s[e];
+        acc[0] = add(acc[0], mul(tv, sv));
+        acc[1] = add(acc[1], mul(tv, tv));
+        acc[2] = add(acc[2], mul(sv, sv));
+    }
+    __device__ void operator()(int k, const double *s3) const {
+        out[k] = s3[0];
+        out[32 + k] = s3[1];
+        out[64 + k] = s3[2];
+    }
+};
+
+// group4 (blas_merged_bicgstab.inl:179-185): r = s - omega*t; rho += r*r0,
+// optionally preceded by the x update of merged_pbicgstab.inl:193
+// (x = alpha_c*p_ + omega_c*s_ + 1*x). The finaliser does lines 207-217:
+// beta = (scal1/rho)*(alpha/omega); rho = scal1; nscal = -(omega*beta);
+// and, for the unpreconditioned form, alpha_c/omega_c from the current iconv
+// (merged_bicgstab.inl:192-199).
+template <int NV, bool XUPD>
+struct EGroup4 {
+    const double *s, *t, *r0;
+    double *r;
+    double *x;
+    const double *pa, *sa;
+    double *sc;
+    template <int NR>
+    __device__ void elem(uint64_t i, int k, double (&acc)[NR]) const {
+        const uint64_t e = i * NV + k;
+        if constexpr (XUPD) {
+            const double ac = sc[SC_ALPHA_C * SC_STRIDE + k], oc = sc[SC_OMEGA_C * SC_STRIDE + k];
+            x[e] = add(add(mul(ac, pa[e]), mul(oc, sa[e])), mul(1.0, x[e]));
+        }
+        const double om = sc[SC_OMEGA * SC_STRIDE + k];
+        const double rv = sub(s[e], mul(om, t[e]));
+        r[e] = rv;
+        acc[0] = add(acc[0], mul(rv, r0[e]));
+    }
+    __device__ void operator()(int k, const double *s1) const {
+        double *S = sc;
+        const double scal1 = s1[0];
+        S[SC_SCAL1 * SC_STRIDE + k] = scal1;
+        const double scal2 = dvd(scal1, S[SC_RHO * SC_STRIDE + k]);
+        const double scal3 = dvd(S[SC_ALPHA * SC_STRIDE + k], S[SC_OMEGA * SC_STRIDE + k]);
+        const double beta = mul(scal2, scal3);
+        S[SC_SCAL2 * SC_STRIDE + k] = scal2;
+        S[SC_SCAL3 * SC_STRIDE + k] = scal3;
+        S[SC_BETA * SC_STRIDE + k] = beta;
+        S[SC_RHO * SC_STRIDE + k] = scal1;
+        S[SC_NSCAL * SC_STRIDE + k] = mul(mul(S[SC_OMEGA * SC_STRIDE + k], beta), -1.0);
+        const double ic = S[SC_ICONV * SC_STRIDE + k];
+        S[SC_ALPHA_C * SC_STRIDE + k] = mul(ic, S[SC_ALPHA * SC_STRIDE + k]);
+        S[SC_OMEGA_C * SC_STRIDE + k] = mul(ic, S[SC_OMEGA * SC_STRIDE + k]);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Flat element-wise kernels (no reduction): one thread per element e of the
+// [n][NV] array, grid-stride.
+// ---------------------------------------------------------------------------
+template <class Op>
+__global__ void __launch_bounds__(CT) k_flat(uint64_t m, Op op) {
+    for (uint64_t e = (uint64_t)blockIdx.x * CT + threadIdx.x; e < m;
+         e += (uint64_t)gridDim.x * CT)
+        op(e);
+}
+
+// s = 1*r + (-alpha)*v  (merged_pbicgstab.inl:159-161)
+struct OpSUpdate {
+    double *s;
+    const double *r, *v, *sc;
+    int nv;
+    __device__ void operator()(uint64_t e) const {
+        const int k = (int)(e % nv);
+        const double na = mul(sc[SC_ALPHA * SC_STRIDE + k], -1.0);
+        s[e] = add(mul(1.0, r[e]), mul(na, v[e]));
+    }
+};
+
+// x = alpha_c*pa + omega_c*sa + 1*x  (merged_pbicgstab.inl:193, blas_ext.inl:173-177)
+struct OpXUpdate {
+    double *x;
+    const double *pa, *sa, *sc;
+    int nv;
+    __device__ void operator()(uint64_t e) const {
+        const int k = (int)(e % nv);
+        const double ac = sc[SC_ALPHA_C * SC_STRIDE + k], oc = sc[SC_OMEGA_C * SC_STRIDE + k];
+        x[e] = add(add(mul(ac, pa[e]), mul(oc, sa[e])), mul(1.0, x[e]));
+    }
+};
+
+// p = 1*r + nscal*v + beta*p  (merged_pbicgstab.inl:216-218)
+struct OpPUpdate {
+    double *p;
+    const double *r, *v, *sc;
+    int nv;
+    __device__ void operator()(uint64_t e) const {
+        const int k = (int)(e % nv);
+        const double ns = sc[SC_NSCAL * SC_STRIDE + k], be = sc[SC_BETA * SC_STRIDE + k];
+        p[e] = add(add(mul(1.0, r[e]), mul(ns, v[e])), mul(be, p[e]));
+    }
+};
+
+// merged_bicgstab_group5 (blas_merged_bicgstab.inl:241-248)
+struct OpGroup5 {
+    double *x, *p;
+    const double *s, *r, *v, *sc;
+    int nv;
+    __device__ void operator()(uint64_t e) const {
+        const int k = (int)(e % nv);
+        const double ac = sc[SC_ALPHA_C * SC_STRIDE + k], oc = sc[SC_OMEGA_C * SC_STRIDE + k];
+        const double be = sc[SC_BETA * SC_STRIDE + k];
+        const double val = mul(be, sc[SC_OMEGA * SC_STRIDE + k]);
+        x[e] = add(x[e], add(mul(ac, p[e]), mul(oc, s[e])));
+        p[e] = sub(add(r[e], mul(be, p[e])), mul(val, v[e]));
+    }
+};
+
+// First Jacobi sweep from x = 0 with r = 0 (blas_merged_jacobi.inl:61-67):
+// x = relax*d*b
+template <typename F>
+struct OpJacobiZero {
+    F *x;
+    const F *b, *d;
+    F relax;
+    int nv;
+    __device__ void operator()(uint64_t e) const {
+        x[e] = mul(mul(relax, d[e / nv]), b[e]);
+    }
+};
+
+template <typename T>
+struct OpFill {
+    T *x;
+    T v;
+    __device__ void operator()(uint64_t e) const { x[e] = v; }
+};
+
+template <typename TD, typename TS>
+struct OpConvert {
+    TD *d;
+    const TS *s;
+    __device__ void operator()(uint64_t e) const { d[e] = (TD)s[e]; }
+};
+
+// y = 1*x + 1*y, or y = 1*x when y is zero-flagged (axpby(a1, x, a1, y))
+template <typename T>
+struct OpAddInto {
+    T *y;
+    const T *x;
+    int y_zero;
+    __device__ void operator()(uint64_t e) const {
+        y[e] = y_zero ? mul(T(1), x[e]) : add(mul(T(1), x[e]), mul(T(1), y[e]));
+    }
+};
+
+// y[i][k] *= d[i]  (blas::scal with an nv = 1 vector, blas.inl:189-193)
+template <typename F>
+struct OpScaleRows {
+    F *y;
+    const F *d;
+    int nv;
+    __device__ void operator()(uint64_t e) const { y[e] = mul(y[e], d[e / nv]); }
+};
+
+// y = a_k*x + 1*y with a_k = coef[k] (axpby(relax, r, a1, x), jacobi.inl:103);
+// y_zero: y = a_k*x (the ax_y branch)
+template <typename F>
+struct OpAxpyK {
+    F *y;
+    const F *x;
+    const double *coef;
+    int nv, y_zero;
+    __device__ void operator()(uint64_t e) const {
+        const F a = (F)coef[e % nv];
+        y[e] = y_zero ? mul(a, x[e]) : add(mul(a, x[e]), mul(F(1), y[e]));
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Hybrid symmetric Gauss-Seidel sweep (csr_gs.inl:77-130) over GS blocks:
+// thread (block g, component k) runs the forward then the backward sweep of
+// rows [off_g, off_g + size_g) with the block-local entries; t already holds
+// b - A_offblock x_old. Blocks are independent, so no thread reads another
+// thread's writes.
+// ---------------------------------------------------------------------------
+template <typename F, typename I, int NV>
+__global__ void __launch_bounds__(CT)
+    k_hsgs_sweep(const uint32_t *__restrict__ row, const I *__restrict__ col,
+                 const F *__restrict__ val, const uint64_t *__restrict__ boff, int nblocks,
+                 const F *__restrict__ t, F *__restrict__ x, const F *__restrict__ d,
+                 const double *__restrict__ relax_sc) {
+    const uint64_t gt = (uint64_t)blockIdx.x * CT + threadIdx.x;
+    const int g = (int)(gt / NV), k = (int)(gt % NV);
+    if (g >= nblocks) return;
+    const uint64_t r0 = boff[g], r1 = boff[g + 1];
+    if (r0 >= r1) return;
+    const F w = (F)relax_sc[k];
+    auto upd = [&](uint64_t i) {
+        const uint64_t e = i * NV + k;
+        F sum = t[e];
+        for (uint32_t j = row[i]; j < row[i + 1]; ++j) {
+            const uint64_t c = (uint64_t)col[j] + r0;
+            sum = sub(sum, mul(x[c * NV + k], val[j]));
+        }
+        const F coeff = mul(w, d[i]);
+        x[e] = add(x[e], mul(coeff, sum));
+    };
+    for (uint64_t i = r0; i < r1; ++i) upd(i);
+    for (uint64_t i = r1; i-- > r0;) upd(i);
+}
+
+// Dense y = A_inv b (dense_matvec.inl:109-117): thread (i, k) accumulates
+// over j in order.
+template <typename F, int NV>
+__global__ void __launch_bounds__(CT)
+    k_dense(const F *__restrict__ a, uint64_t n, const F *__restrict__ x, F *__restrict__ y) {
+    const uint64_t e = (uint64_t)blockIdx.x * CT + threadIdx.x;
+    if (e >= n * NV) return;
+    const uint64_t i = e / NV;
+    const int k = (int)(e % NV);
+    F acc = F(0);
+    const F *ar = a + i * n;
+    for (uint64_t j = 0; j < n; ++j) acc = add(acc, mul(__ldg(&ar[j]), x[j * NV + k]));
+    y[e] = acc;
+}
+
+}  // namespace k
+}  // namespace xg

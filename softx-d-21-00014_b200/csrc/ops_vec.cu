@@ -1,0 +1,174 @@
+// Flat element-wise launchers, the process context, and CSR upload/download
+// with XAMG's index narrowing.
+#include <cstring>
+
+#include "ops.h"
+
+namespace xg {
+
+static Ctx g_ctx;
+uint64_t g_kernel_launches = 0;
+
+Ctx &ctx() {
+    if (!g_ctx.ready) g_ctx.init();
+    return g_ctx;
+}
+
+Ctx &ctx_uninit() { return g_ctx; }
+
+void Ctx::init() {
+    if (ready) return;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        throw Error(XAMG_ERR_CUDA, std::string("no CUDA device available: ") +
+                                       (e != cudaSuccess ? cudaGetErrorString(e) : "0 devices"));
+    if (device_request >= 0) XG_CUDA(cudaSetDevice(device_request));
+    XG_CUDA(cudaGetDevice(&device));
+    XG_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    red_part.alloc((size_t)k::BMAX * 32 * 3 * sizeof(double));
+    red_ticket.alloc(sizeof(unsigned) * 4);
+    red_out.alloc(128 * sizeof(double));
+    XG_CUDA(cudaMemsetAsync(red_ticket.p, 0, red_ticket.bytes, stream));
+    XG_CUDA(cudaMallocHost((void **)&pinned, 256 * sizeof(double)));
+    XG_CUDA(cudaStreamSynchronize(stream));
+    ready = true;
+}
+
+void Ctx::shutdown() {
+    if (!ready) return;
+    cudaStreamSynchronize(stream);
+    red_part.release();
+    red_ticket.release();
+    red_out.release();
+    if (pinned) cudaFreeHost(pinned);
+    pinned = nullptr;
+    cudaStreamDestroy(stream);
+    stream = nullptr;
+    ready = false;
+}
+
+namespace ops {
+
+template <class Op>
+static void flat(uint64_t m, const Op &op, cudaStream_t s) {
+    if (m == 0) return;
+    uint64_t blocks = (m + k::CT - 1) / k::CT;
+    if (blocks > (uint64_t)k::BMAX * 4) blocks = (uint64_t)k::BMAX * 4;
+    k::k_flat<Op><<<(unsigned)blocks, k::CT, 0, s>>>(m, op);
+    XG_CUDA(cudaGetLastError());
+    ++g_kernel_launches;
+}
+
+void s_update(uint64_t n, double *s_, const double *r, const double *v, const double *sc, int nv,
+              cudaStream_t s) {
+    flat(n * nv, k::OpSUpdate{s_, r, v, sc, nv}, s);
+}
+void x_update(uint64_t n, double *x, const double *pa, const double *sa, const double *sc,
+              int nv, cudaStream_t s) {
+    flat(n * nv, k::OpXUpdate{x, pa, sa, sc, nv}, s);
+}
+void p_update(uint64_t n, double *p, const double *r, const double *v, const double *sc, int nv,
+              cudaStream_t s) {
+    flat(n * nv, k::OpPUpdate{p, r, v, sc, nv}, s);
+}
+void group5(uint64_t n, double *x, double *p, const double *s_, const double *r, const double *v,
+            const double *sc, int nv, cudaStream_t s) {
+    flat(n * nv, k::OpGroup5{x, p, s_, r, v, sc, nv}, s);
+}
+
+template <typename F>
+void jacobi_zero(uint64_t n, F *x, const F *b, const F *d, F relax, int nv, cudaStream_t s) {
+    flat(n * nv, k::OpJacobiZero<F>{x, b, d, relax, nv}, s);
+}
+template void jacobi_zero<double>(uint64_t, double *, const double *, const double *, double, int,
+                                  cudaStream_t);
+template void jacobi_zero<float>(uint64_t, float *, const float *, const float *, float, int,
+                                 cudaStream_t);
+
+template <typename T>
+void fill(T *x, uint64_t m, T v, cudaStream_t s) {
+    flat(m, k::OpFill<T>{x, v}, s);
+}
+template void fill<double>(double *, uint64_t, double, cudaStream_t);
+template void fill<float>(float *, uint64_t, float, cudaStream_t);
+
+template <typename TD, typename TS>
+void convert(TD *d, const TS *src, uint64_t m, cudaStream_t s) {
+    flat(m, k::OpConvert<TD, TS>{d, src}, s);
+}
+template void convert<float, double>(float *, const double *, uint64_t, cudaStream_t);
+template void convert<double, float>(double *, const float *, uint64_t, cudaStream_t);
+template void convert<double, double>(double *, const double *, uint64_t, cudaStream_t);
+template void convert<float, float>(float *, const float *, uint64_t, cudaStream_t);
+
+template <typename T>
+void add_into(T *y, const T *x, uint64_t m, bool y_zero, cudaStream_t s) {
+    flat(m, k::OpAddInto<T>{y, x, (int)y_zero}, s);
+}
+template void add_into<double>(double *, const double *, uint64_t, bool, cudaStream_t);
+template void add_into<float>(float *, const float *, uint64_t, bool, cudaStream_t);
+
+template <typename F>
+void scale_rows(F *y, const F *d, uint64_t n, int nv, cudaStream_t s) {
+    flat(n * nv, k::OpScaleRows<F>{y, d, nv}, s);
+}
+template void scale_rows<double>(double *, const double *, uint64_t, int, cudaStream_t);
+template void scale_rows<float>(float *, const float *, uint64_t, int, cudaStream_t);
+
+template <typename F>
+void axpy_k(F *y, const F *x, const double *coef, uint64_t n, int nv, bool y_zero,
+            cudaStream_t s) {
+    flat(n * nv, k::OpAxpyK<F>{y, x, coef, nv, (int)y_zero}, s);
+}
+template void axpy_k<double>(double *, const double *, const double *, uint64_t, int, bool,
+                             cudaStream_t);
+template void axpy_k<float>(float *, const float *, const double *, uint64_t, int, bool,
+                            cudaStream_t);
+
+}  // namespace ops
+
+// ---------------------------------------------------------------------------
+// CSR upload with XAMG's narrowing (matrix_block::assemble, matrix.h:78-93:
+// hash from encode_hash, values converted to float when reduced).
+// ---------------------------------------------------------------------------
+void upload_csr(const HCsr &h, DCsr &d, bool f32, bool narrow, cudaStream_t s) {
+    d.nrows = h.nrows;
+    d.ncols = h.ncols;
+    d.nnz = h.nnz();
+    d.f32 = f32;
+    d.hash = encode_hash(d.nnz, d.ncols, d.nrows, d.ncols, false, f32);
+    const uint16_t i2 = define_int_type(d.ncols);
+    d.col_bytes = narrow ? int_type_bytes(i2 > I32_TYPE ? I32_TYPE : i2) : 4;
+    XG_REQUIRE(d.ncols <= UINT32_MAX && d.nnz <= UINT32_MAX, XAMG_ERR_UNSUPPORTED,
+               "matrix exceeds 32-bit indexing");
+    upload(d.row, h.row, s);
+    if (d.col_bytes == 4) {
+        upload(d.col, h.col, s);
+    } else if (d.col_bytes == 2) {
+        std::vector<uint16_t> c(h.col.begin(), h.col.end());
+        upload(d.col, c, s);
+        XG_CUDA(cudaStreamSynchronize(s));
+    } else {
+        std::vector<uint8_t> c(h.col.begin(), h.col.end());
+        upload(d.col, c, s);
+        XG_CUDA(cudaStreamSynchronize(s));
+    }
+    if (f32) {
+        std::vector<float> v(h.val.size());
+        for (size_t i = 0; i < v.size(); ++i) v[i] = (float)h.val[i];
+        upload(d.val, v, s);
+        XG_CUDA(cudaStreamSynchronize(s));
+    } else {
+        upload(d.val, h.val, s);
+    }
+    XG_CUDA(cudaStreamSynchronize(s));
+}
+
+void download_csr(const DCsr &d, uint32_t *row, void *col, void *val) {
+    if (row && d.row.bytes) XG_CUDA(cudaMemcpy(row, d.row.p, d.row.bytes, cudaMemcpyDeviceToHost));
+    if (col && d.col.bytes) XG_CUDA(cudaMemcpy(col, d.col.p, d.col.bytes, cudaMemcpyDeviceToHost));
+    if (val && d.val.bytes) XG_CUDA(cudaMemcpy(val, d.val.p, d.val.bytes, cudaMemcpyDeviceToHost));
+}
+
+}  // namespace xg

@@ -1,0 +1,774 @@
+// Solver objects (see solver.h). Each solve() restates the reference
+// solver's control flow; the comments name the reference lines.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "host_num.h"
+#include "ops.h"
+#include "solver.h"
+
+namespace xg {
+
+static cudaStream_t S() { return ctx().stream; }
+
+void SolverBase::reset_stats() {
+    // solver_stats::reset (solver.h:54-65)
+    st.iters = 0;
+    if ((int)st.conv.size() != NV) {
+        st.conv.assign(NV, 0);
+        st.abs_res.assign(NV, 0.0);
+        st.rel_res.assign(NV, 0.0);
+    }
+    if (cfg.convergence_check) {
+        std::fill(st.conv.begin(), st.conv.end(), 0);
+        std::fill(st.abs_res.begin(), st.abs_res.end(), 0.0);
+        std::fill(st.rel_res.begin(), st.rel_res.end(), 0.0);
+    }
+}
+
+void SolverBase::alloc_buffers(int count) {
+    buf.resize(count);
+    for (auto &v : buf) v.alloc(n, NV, f32);
+}
+
+// Residual table (io/detail/print.inl:41-111)
+static void print_header(int nv) {
+    printf("%s |\n", std::string(10 + nv * 30, '-').c_str());
+    printf("%7s | ", "Iter");
+    for (int i = 0; i < nv; ++i) printf("%12s | %12s | ", "res", "res / res0");
+    printf("\n");
+}
+static void print_row(int it, const double *res, const double *res0,
+                      const std::vector<double> &conv) {
+    printf("%7d | ", it);
+    for (size_t k = 0; k < conv.size(); ++k) {
+        if (conv[k] != 0)
+            printf("%12e | %12e | ", std::sqrt(res[k]), std::sqrt(res[k] / res0[k]));
+        else
+            printf("%12s | %12s | ", "-", "-");
+    }
+    printf("\n");
+}
+
+// base_solver::convergence_check + converged + convergence_status
+// (solver.h:173-241): tolerances are float32, compared against double norms.
+static bool host_converged(SolverBase &sv, const double *res, const double *res0,
+                           std::vector<double> &iconv) {
+    if (!sv.cfg.convergence_check) return false;
+    if (sv.cfg.convergence_info) {
+        if (!sv.st.iters) print_header(sv.NV);
+        print_row(sv.st.iters, res, res0, iconv);
+    }
+    const float abs_tol = sv.cfg.abs_tol, rel_tol = sv.cfg.rel_tol;
+    bool flag = true;
+    for (int k = 0; k < sv.NV; ++k) {
+        if (iconv[k] != 0) {
+            const double a = std::sqrt(res[k]);
+            const double r = a / std::sqrt(res0[k]);
+            if ((a > abs_tol) && (r > rel_tol)) {
+                flag = false;
+            } else if (!sv.st.conv[k]) {
+                sv.st.abs_res[k] = a;
+                sv.st.rel_res[k] = r;
+                sv.st.conv[k] = 1;
+            }
+        }
+    }
+    if (flag) {
+        if (sv.cfg.convergence_info) printf("%s |\n", std::string(10 + sv.NV * 30, '-').c_str());
+        return true;
+    }
+    for (int k = 0; k < sv.NV; ++k) iconv[k] *= (double)(!sv.st.conv[k]);
+    return false;
+}
+
+// Reads nv doubles of device scalars into host memory (synchronises).
+static void read_scalars(const double *dev, double *host, int nv) {
+    Ctx &c = ctx();
+    XG_CUDA(cudaMemcpyAsync(c.pinned, dev, nv * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    XG_CUDA(cudaStreamSynchronize(c.stream));
+    std::memcpy(host, c.pinned, nv * sizeof(double));
+}
+
+// get_residual (solver.h:243-256) with the norm into res (host)
+template <typename F>
+static void residual_norm(const DCsr &A, DVec &x, DVec &b, DVec &r, int nv, double *res_host) {
+    double *dn = ctx().red_out.as<double>();
+    if (x.zero) {
+        // Ax_y leaves r zero-flagged; axpby(1, b, -1, r) takes its ax_y branch: r = 1*b
+        ops::convert<F, F>(r.p<F>(), b.p<F>(), r.elems(), S());
+        ops::dot<F>(r.n, r.p<F>(), r.p<F>(), dn, nv, S());
+    } else {
+        ops::residual<F>(A, x.p<F>(), b.p<F>(), r.p<F>(), nv, dn, S());
+    }
+    r.zero = false;
+    r.init = true;
+    read_scalars(dn, res_host, nv);
+}
+
+// ===========================================================================
+// Jacobi (jacobi.inl:49-120)
+// ===========================================================================
+template <typename F>
+struct Jacobi : public SolverBase {
+    DevBuf d;  // inverse diagonal, level precision
+    DevBuf relax_dev;
+    void setup_from(const HCsr &hA) {
+        if (f32)
+            upload(d, inv_diag_f32(hA, false), S());
+        else
+            upload(d, inv_diag_f64(hA, false), S());
+        alloc_buffers(2);
+        relax_dev.alloc(32 * sizeof(double));
+        XG_CUDA(cudaStreamSynchronize(S()));
+    }
+    void solve(DVec &x, DVec &b, const std::vector<double> &conv) override {
+        reset_stats();
+        const F relax = (F)cfg.relax;
+        const int m = std::max(1, cfg.max_iters);
+        if (cfg.convergence_check) {
+            solve_checked(x, b, conv);
+            return;
+        }
+        // x_out alternates between x and buf[1]; sweep j lands in x when
+        // (m - j) is even so that the last one does.
+        DVec &T = buf[1];
+        auto tgt = [&](int j) -> DVec & { return ((m - j) % 2 == 0) ? x : T; };
+        DVec *cur = &x;
+        int j = 1;
+        if (x.zero) {
+            DVec &o = tgt(1);
+            ops::jacobi_zero<F>(n, o.p<F>(), b.p<F>(), d.as<F>(), relax, NV, S());
+            cur = &o;
+            j = 2;
+        } else if ((m - 1) % 2 == 0) {
+            ops::convert<F, F>(T.p<F>(), x.p<F>(), x.elems(), S());
+            cur = &T;
+        }
+        for (; j <= m; ++j) {
+            DVec &o = tgt(j);
+            ops::jacobi_sweep<F>(*A, cur->p<F>(), o.p<F>(), b.p<F>(), d.as<F>(), relax, NV, S());
+            cur = &o;
+        }
+        st.iters = m;
+        x.zero = false;
+        x.init = true;
+    }
+    // jacobi.inl:93-112
+    void solve_checked(DVec &x, DVec &b, const std::vector<double> &conv) {
+        std::vector<double> iconv = conv, rho0(NV), res(NV), relax_h(NV, (double)(F)cfg.relax);
+        DVec &r = buf[0];
+        residual_norm<F>(*A, x, b, r, NV, rho0.data());
+        if (host_converged(*this, rho0.data(), rho0.data(), iconv)) return;
+        do {
+            ++st.iters;
+            ops::scale_rows<F>(r.p<F>(), d.as<F>(), n, NV, S());
+            for (int k = 0; k < NV; ++k) relax_h[k] = (double)(F)(relax_h[k] * iconv[k]);
+            XG_CUDA(cudaMemcpyAsync(relax_dev.p, relax_h.data(), NV * sizeof(double),
+                                    cudaMemcpyHostToDevice, S()));
+            ops::axpy_k<F>(x.p<F>(), r.p<F>(), relax_dev.as<double>(), n, NV, x.zero, S());
+            x.zero = false;
+            residual_norm<F>(*A, x, b, r, NV, res.data());
+            if (host_converged(*this, res.data(), rho0.data(), iconv)) return;
+        } while (st.iters < cfg.max_iters);
+    }
+};
+
+// ===========================================================================
+// Hybrid symmetric Gauss-Seidel (hsgs.inl:50-115, blas2.h:184-281,
+// csr_gs.inl:32-134). GS blocks play the role of XAMG's cores: rows are split
+// with XAMG's core rule into nb = max(1, n / gpu_hsgs_rows) blocks; entries
+// coupling a block to another one are lagged (use x from before the sweep).
+// ===========================================================================
+template <typename F>
+struct Hsgs : public SolverBase {
+    DevBuf d, boff, relax_dev;
+    DCsr Adiag, Aoff;
+    int nblocks = 1;
+    void setup_from(const HCsr &hA) {
+        const uint64_t rows = cfg.gpu_hsgs_rows > 0 ? (uint64_t)cfg.gpu_hsgs_rows : 32;
+        nblocks = (int)std::max<uint64_t>(1, n / rows);
+        const uint64_t cs = split_range_f64(n, nblocks);
+        std::vector<uint64_t> off(nblocks + 1);
+        for (int c = 0; c <= nblocks; ++c) off[c] = std::min<uint64_t>(n, cs * (uint64_t)c);
+        off[nblocks] = n;
+        // block id of every row
+        std::vector<uint32_t> bid(n);
+        for (int c = 0; c < nblocks; ++c)
+            for (uint64_t i = off[c]; i < off[c + 1]; ++i) bid[i] = c;
+        HCsr dg, od;
+        dg.nrows = od.nrows = n;
+        od.ncols = n;
+        uint64_t maxb = 1;
+        for (int c = 0; c < nblocks; ++c) maxb = std::max<uint64_t>(maxb, off[c + 1] - off[c]);
+        dg.ncols = maxb;
+        dg.row.assign(n + 1, 0);
+        od.row.assign(n + 1, 0);
+        std::vector<std::pair<uint32_t, uint64_t>> tmp;
+        for (uint64_t i = 0; i < n; ++i) {
+            const uint32_t c = bid[i];
+            tmp.clear();
+            for (uint64_t j = hA.row[i]; j < hA.row[i + 1]; ++j) {
+                const uint32_t col = hA.col[j];
+                if (bid[col] == c) {
+                    dg.col.push_back((uint32_t)(col - off[c]));
+                    dg.val.push_back(hA.val[j]);
+                } else {
+                    tmp.push_back({bid[col], j});
+                }
+            }
+            // off-core chunks are visited in block order, entries in row order
+            std::stable_sort(tmp.begin(), tmp.end(),
+                             [](const std::pair<uint32_t, uint64_t> &a,
+                                const std::pair<uint32_t, uint64_t> &b) { return a.first < b.first; });
+            for (auto &t : tmp) {
+                od.col.push_back(hA.col[t.second]);
+                od.val.push_back(hA.val[t.second]);
+            }
+            dg.row[i + 1] = (uint32_t)dg.col.size();
+            od.row[i + 1] = (uint32_t)od.col.size();
+        }
+        upload_csr(dg, Adiag, f32, cfg.gpu_index_compress != 0, S());
+        upload_csr(od, Aoff, f32, cfg.gpu_index_compress != 0, S());
+        upload(boff, off, S());
+        if (f32)
+            upload(d, inv_diag_f32(hA, false), S());
+        else
+            upload(d, inv_diag_f64(hA, false), S());
+        relax_dev.alloc(32 * sizeof(double));
+        std::vector<double> rh(32, (double)(F)cfg.relax);
+        XG_CUDA(cudaMemcpy(relax_dev.p, rh.data(), 32 * sizeof(double), cudaMemcpyHostToDevice));
+        alloc_buffers(2);
+        XG_CUDA(cudaStreamSynchronize(S()));
+    }
+    void solve(DVec &x, DVec &b, const std::vector<double> &conv) override {
+        reset_stats();
+        std::vector<double> iconv = conv, rho0(NV), res(NV);
+        std::vector<double> relax_h(NV, (double)(F)cfg.relax);
+        bool ones = true;
+        for (int k = 0; k < NV; ++k) ones = ones && (iconv[k] == 1.0);
+        DVec &r = buf[0];
+        DVec &t = buf[1];
+        if (cfg.convergence_check) {
+            residual_norm<F>(*A, x, b, r, NV, rho0.data());
+            if (host_converged(*this, rho0.data(), rho0.data(), iconv)) return;
+        }
+        do {
+            ++st.iters;
+            // scal(iconv, relax_conv) (hsgs.inl:102)
+            if (!ones || cfg.convergence_check) {
+                for (int k = 0; k < NV; ++k) relax_h[k] = (double)(F)(relax_h[k] * iconv[k]);
+                XG_CUDA(cudaMemcpyAsync(relax_dev.p, relax_h.data(), NV * sizeof(double),
+                                        cudaMemcpyHostToDevice, S()));
+            }
+            if (x.zero) {
+                // no lagged term: t = 1*b + (-1)*0 = b; x = 0 (blas2.h:226-262)
+                ops::convert<F, F>(t.p<F>(), b.p<F>(), t.elems(), S());
+                ops::fill<F>(x.p<F>(), x.elems(), F(0), S());
+            } else {
+                ops::residual<F>(Aoff, x.p<F>(), b.p<F>(), t.p<F>(), NV, nullptr, S());
+            }
+            ops::hsgs_sweep<F>(Adiag, boff.as<uint64_t>(), nblocks, t.p<F>(), x.p<F>(), d.as<F>(),
+                               relax_dev.as<double>(), NV, S());
+            x.zero = false;
+            x.init = true;
+            if (cfg.convergence_check) {
+                residual_norm<F>(*A, x, b, r, NV, res.data());
+                if (host_converged(*this, res.data(), rho0.data(), iconv)) return;
+            }
+        } while (st.iters < cfg.max_iters);
+    }
+};
+
+// ===========================================================================
+// Chebyshev (chebyshev.inl:129-206)
+// ===========================================================================
+template <typename F>
+struct Chebyshev : public SolverBase {
+    DevBuf isd;
+    double min_eig = 0, max_eig = 0;
+    std::vector<F> coef;
+    void setup_from(const HCsr &hA) {
+        if (f32)
+            upload(isd, inv_diag_f32(hA, true), S());
+        else
+            upload(isd, inv_diag_f64(hA, true), S());
+        alloc_buffers(3);
+        XG_CUDA(cudaStreamSynchronize(S()));
+    }
+    void solve(DVec &x, DVec &b, const std::vector<double> &conv) override {
+        reset_stats();
+        const int order = cfg.poly_order;
+        XG_REQUIRE(order >= 1 && order <= 4, XAMG_ERR_INVALID_ARG,
+                   "Chebyshev polynomial_order must be 1..4");
+        std::vector<double> cd = cheby_coeffs(min_eig, max_eig, order, (double)cfg.spec_fraction);
+        coef.resize(order);
+        for (int i = 0; i < order; ++i) coef[i] = (F)cd[i];
+        std::vector<double> rho0(NV), res(NV);
+        const bool x_zero = x.zero;
+        if (cfg.convergence_check && cfg.convergence_info) {
+            residual_norm<F>(*A, x, b, buf[0], NV, rho0.data());
+            print_header(NV);
+            print_row(0, rho0.data(), rho0.data(), conv);
+        }
+        DVec &rs = buf[0];
+        DVec *t1s = &buf[1], *other = &buf[2];
+        ops::cheby_first<F>(*A, x.p<F>(), x_zero, b.p<F>(), isd.as<F>(), coef[order - 1],
+                            rs.p<F>(), t1s->p<F>(), NV, S());
+        if (order == 1) {
+            ops::add_into<F>(x.p<F>(), t1s->p<F>(), x.elems(), x_zero, S());
+        } else {
+            for (int i = order - 2; i >= 0; --i) {
+                const bool last = (i == 0);
+                DVec &out = last ? x : *other;
+                ops::cheby_step<F>(*A, t1s->p<F>(), rs.p<F>(), isd.as<F>(), coef[i], out.p<F>(),
+                                   last, x_zero, NV, S());
+                if (!last) std::swap(t1s, other);
+            }
+        }
+        x.zero = false;
+        x.init = true;
+        if (cfg.convergence_check && cfg.convergence_info) {
+            residual_norm<F>(*A, x, b, buf[0], NV, res.data());
+            print_row(0, res.data(), rho0.data(), conv);
+        }
+    }
+};
+
+// ===========================================================================
+// Direct coarse solve (direct.inl:31-56): dense Gauss-Jordan inverse built on
+// the host at setup, applied as a dense multi-RHS product.
+// ===========================================================================
+template <typename F>
+struct Direct : public SolverBase {
+    DevBuf inv;
+    void setup_from(const HCsr &hA) {
+        if (f32)
+            upload(inv, dense_inverse_f32(hA), S());
+        else
+            upload(inv, dense_inverse_f64(hA), S());
+        XG_CUDA(cudaStreamSynchronize(S()));
+    }
+    void solve(DVec &x, DVec &b, const std::vector<double> &) override {
+        // blas2::Ax_y short-circuit on a zero-flagged input (blas2.h:309-313)
+        if (b.zero) {
+            x.zero = true;
+            return;
+        }
+        ops::dense_apply<F>(inv.as<F>(), n, b.p<F>(), x.p<F>(), NV, S());
+        x.zero = false;
+        x.init = true;
+    }
+};
+
+// Identity (solver.h:340-368): x = b
+template <typename F>
+struct Identity : public SolverBase {
+    void solve(DVec &x, DVec &b, const std::vector<double> &) override {
+        if (b.zero) {
+            x.zero = true;
+            x.init = true;
+            return;
+        }
+        ops::convert<F, F>(x.p<F>(), b.p<F>(), x.elems(), S());
+        x.zero = false;
+        x.init = true;
+    }
+};
+
+template <typename F>
+static std::unique_ptr<SolverBase> make_smoother_t(const SolverCfg &cfg, const std::string &role,
+                                                   const DCsr &A, const HCsr &hA, int nv,
+                                                   double min_eig, double max_eig) {
+    std::unique_ptr<SolverBase> s;
+    const std::string &m = cfg.method;
+    auto init = [&](SolverBase *b) {
+        b->cfg = cfg;
+        b->role = role;
+        b->NV = nv;
+        b->f32 = std::is_same<F, float>::value;
+        b->A = &A;
+        b->n = A.nrows;
+    };
+    if (m == "Jacobi") {
+        auto *j = new Jacobi<F>();
+        init(j);
+        j->setup_from(hA);
+        s.reset(j);
+    } else if (m == "HSGS") {
+        auto *h = new Hsgs<F>();
+        init(h);
+        h->setup_from(hA);
+        s.reset(h);
+    } else if (m == "Chebyshev") {
+        auto *c = new Chebyshev<F>();
+        init(c);
+        c->min_eig = min_eig;
+        c->max_eig = max_eig;
+        c->setup_from(hA);
+        s.reset(c);
+    } else if (m == "Direct") {
+        auto *d = new Direct<F>();
+        init(d);
+        d->setup_from(hA);
+        s.reset(d);
+    } else if (m == "Identity") {
+        auto *d = new Identity<F>();
+        init(d);
+        s.reset(d);
+    } else {
+        throw Error(XAMG_ERR_UNSUPPORTED, "method '" + m + "' cannot be used as " + role);
+    }
+    return s;
+}
+
+std::unique_ptr<SolverBase> make_smoother(const SolverCfg &cfg, const std::string &role,
+                                          const DCsr &A, const HCsr &hA, bool f32, int nv,
+                                          double min_eig, double max_eig) {
+    if (f32) return make_smoother_t<float>(cfg, role, A, hA, nv, min_eig, max_eig);
+    return make_smoother_t<double>(cfg, role, A, hA, nv, min_eig, max_eig);
+}
+
+// ===========================================================================
+// MultiGrid (mg.inl:97-334)
+// ===========================================================================
+void MultiGrid::build(const HCsr &A0, const DCsr *A0dev, const Params &P, const std::string &rl,
+                      int nv) {
+    role = rl;
+    NV = nv;
+    cfg = resolve_cfg(P.get(role), role);
+    A = A0dev;
+    n = A0.nrows;
+    f32 = false;
+    H = build_hierarchy(A0, cfg);
+    const int nl = (int)H.lv.size();
+    XG_REQUIRE(nl >= 2, XAMG_ERR_UNSUPPORTED, "multigrid hierarchy has fewer than 2 levels");
+    const bool reduced = cfg.gpu_precond_f32 >= 0 ? cfg.gpu_precond_f32 != 0
+                                                  : cfg.mg_reduced_precision != 0;
+    const bool narrow = cfg.gpu_index_compress != 0;
+    L.clear();
+    L.resize(nl);
+    for (int l = 0; l < nl; ++l) {
+        MgLevel &lv = L[l];
+        lv.f32 = (l >= 1) && reduced;
+        lv.tf32 = reduced;
+        lv.min_eig = H.lv[l].min_eig;
+        lv.max_eig = H.lv[l].max_eig;
+        if (l >= 1) upload_csr(H.lv[l].A, lv.A, lv.f32, narrow, S());
+        if (l + 1 < nl) {
+            // R = P^T (hypre_base.inl:400-401, transpose.inl:31-108)
+            const HCsr &Ph = H.lv[l].P;
+            HCsr R;
+            R.nrows = Ph.ncols;
+            R.ncols = Ph.nrows;
+            std::vector<uint32_t> cnt(Ph.ncols + 1, 0);
+            for (uint32_t c : Ph.col) ++cnt[c + 1];
+            R.row.assign(Ph.ncols + 1, 0);
+            for (uint64_t c = 0; c < Ph.ncols; ++c) R.row[c + 1] = R.row[c] + cnt[c + 1];
+            R.col.resize(Ph.nnz());
+            R.val.resize(Ph.nnz());
+            std::vector<uint32_t> pos(R.row.begin(), R.row.end() - 1);
+            for (uint64_t i = 0; i < Ph.nrows; ++i)
+                for (uint64_t j = Ph.row[i]; j < Ph.row[i + 1]; ++j) {
+                    const uint32_t c = Ph.col[j];
+                    R.col[pos[c]] = (uint32_t)i;
+                    R.val[pos[c]] = Ph.val[j];
+                    ++pos[c];
+                }
+            upload_csr(Ph, lv.P, lv.tf32, narrow, S());
+            upload_csr(R, lv.R, lv.tf32, narrow, S());
+        }
+        const uint64_t nrow = H.lv[l].A.nrows;
+        if (l == 0) {
+            lv.temp.alloc(nrow, nv, false);
+        } else {
+            lv.temp.alloc(nrow, nv, lv.f32);
+            lv.bH.alloc(nrow, nv, lv.f32);
+            lv.xH.alloc(nrow, nv, lv.f32);
+        }
+    }
+    pre.clear();
+    post.clear();
+    for (int l = 0; l + 1 < nl; ++l) {
+        const DCsr &Al = (l == 0) ? *A0dev : L[l].A;
+        SolverCfg pc = resolve_cfg(P.get("pre_smoother", l), "pre_smoother");
+        SolverCfg qc = resolve_cfg(P.get("post_smoother", l), "post_smoother");
+        pc.gpu_index_compress = qc.gpu_index_compress = cfg.gpu_index_compress;
+        pre.push_back(make_smoother(pc, "pre_smoother", Al, H.lv[l].A, L[l].f32, nv,
+                                    L[l].min_eig, L[l].max_eig));
+        post.push_back(make_smoother(qc, "post_smoother", Al, H.lv[l].A, L[l].f32, nv,
+                                     L[l].min_eig, L[l].max_eig));
+    }
+    SolverCfg cc = resolve_cfg(P.get("coarse_grid_solver"), "coarse_grid_solver");
+    coarse = make_smoother(cc, "coarse_grid_solver", L[nl - 1].A, H.lv[nl - 1].A, L[nl - 1].f32,
+                           nv, L[nl - 1].min_eig, L[nl - 1].max_eig);
+    buf.resize(1);
+    buf[0].alloc(n, nv, false);
+    XG_CUDA(cudaStreamSynchronize(S()));
+}
+
+// mg.inl:166-260
+void MultiGrid::cycle(int level, DVec &x, DVec &b, int cyc, const std::vector<double> &iconv) {
+    MgLevel &lv = L[level];
+    const DCsr &Al = (level == 0) ? *A : lv.A;
+    const int nl = (int)L.size();
+    MgLevel &nx = L[level + 1];
+    DVec &temp = lv.temp, &bH = nx.bH, &xH = nx.xH;
+    const bool mixed = (lv.f32 != nx.f32);  // level 0 -> 1 with reduced precision
+    if (cyc != 1) pre[level]->solve(x, b, iconv);
+    // residual temp = b - A x (Ax_y + axpby(a1, b, a_1, temp))
+    const DVec *rin = &temp;
+    if (x.zero) {
+        rin = &b;  // temp = 1*b, bitwise b
+    } else if (lv.f32) {
+        ops::residual<float>(Al, x.p<float>(), b.p<float>(), temp.p<float>(), NV, nullptr, S());
+    } else {
+        ops::residual<double>(Al, x.p<double>(), b.p<double>(), temp.p<double>(), NV, nullptr,
+                              S());
+    }
+    // restriction (with the float conversion fused when the precision changes)
+    if (b.zero && x.zero) {
+        bH.zero = true;
+    } else if (mixed) {
+        ops::spmv_f32_from_f64(lv.R, rin->p<double>(), bH.p<float>(), NV, S());
+        bH.zero = false;
+    } else if (nx.f32) {
+        ops::spmv<float>(lv.R, rin->p<float>(), bH.p<float>(), NV, false, S());
+        bH.zero = false;
+    } else {
+        ops::spmv<double>(lv.R, rin->p<double>(), bH.p<double>(), NV, false, S());
+        bH.zero = false;
+    }
+    bH.init = true;
+    xH.zero = true;  // set_const(x_H, 0)
+    xH.init = true;
+    if (level + 1 == nl - 1) {
+        coarse->solve(xH, bH, iconv);
+    } else {
+        cycle(level + 1, xH, bH, cyc, iconv);
+        if (cyc == 2)
+            cycle(level + 1, xH, bH, 2, iconv);
+        else if (cyc == 1)
+            cycle(level + 1, xH, bH, 0, iconv);
+    }
+    // prolongation
+    if (!xH.zero) {
+        if (mixed) {
+            ops::prolong_mixed(lv.P, xH.p<float>(), x.p<double>(), x.zero, NV, S());
+        } else {
+            // Axpy(P, x_H, x) accumulates into x; a zero-flagged x is written
+            // with zeros first so that no stale contents are read
+            if (x.zero) {
+                if (lv.f32)
+                    ops::fill<float>(x.p<float>(), x.elems(), 0.f, S());
+                else
+                    ops::fill<double>(x.p<double>(), x.elems(), 0.0, S());
+            }
+            if (lv.f32)
+                ops::spmv<float>(lv.P, xH.p<float>(), x.p<float>(), NV, true, S());
+            else
+                ops::spmv<double>(lv.P, xH.p<double>(), x.p<double>(), NV, true, S());
+        }
+        x.zero = false;
+        x.init = true;
+    }
+    post[level]->solve(x, b, iconv);
+}
+
+// mg.inl:262-334
+void MultiGrid::solve(DVec &x, DVec &b, const std::vector<double> &conv) {
+    reset_stats();
+    std::vector<double> iconv = conv, rho0(NV), res(NV);
+    DVec &r = buf[0];
+    if (cfg.convergence_check) {
+        residual_norm<double>(*A, x, b, r, NV, rho0.data());
+        if (host_converged(*this, rho0.data(), rho0.data(), iconv)) return;
+    }
+    do {
+        ++st.iters;
+        cycle(0, x, b, cfg.mg_cycle, iconv);
+        if (cfg.convergence_check) {
+            residual_norm<double>(*A, x, b, r, NV, res.data());
+            if (host_converged(*this, res.data(), rho0.data(), iconv)) return;
+        }
+    } while (st.iters < cfg.max_iters);
+}
+
+// ===========================================================================
+// BiCGStab family (merged_pbicgstab.inl:44-225, merged_bicgstab.inl:44-208,
+// pbicgstab.inl, bicgstab.inl)
+// ===========================================================================
+void Krylov::setup() {
+    alloc_buffers(8);
+    sc.alloc(k::SC_COUNT * k::SC_STRIDE * sizeof(double));
+    XG_CUDA(cudaMemset(sc.p, 0, sc.bytes));
+}
+
+void Krylov::upload_iconv(const std::vector<double> &iconv) {
+    std::vector<double> h(iconv);
+    XG_CUDA(cudaMemcpyAsync(sc.as<double>() + k::SC_ICONV * k::SC_STRIDE, h.data(),
+                            NV * sizeof(double), cudaMemcpyHostToDevice, S()));
+}
+
+bool Krylov::check(const double *res, const double *res0, std::vector<double> &iconv) {
+    const std::vector<double> before = iconv;
+    const bool done = host_converged(*this, res, res0, iconv);
+    if (!done && iconv != before) upload_iconv(iconv);
+    return done;
+}
+
+void Krylov::apply_M(DVec &out, DVec &in) {
+    // set_const(out, 0) then precond->solve(out, in) with conv = ones
+    out.zero = true;
+    out.init = true;
+    static const std::vector<double> ones(32, 1.0);
+    std::vector<double> o(ones.begin(), ones.begin() + NV);
+    M->solve(out, in, o);
+}
+
+void Krylov::solve(DVec &x, DVec &b, const std::vector<double> &conv) {
+    reset_stats();
+    cudaStream_t s = S();
+    std::vector<double> iconv = conv;
+    upload_iconv(iconv);
+    double *SC = sc.as<double>();
+    for (auto &v : buf) {
+        v.zero = true;
+        v.init = true;
+    }
+    DVec &r0 = buf[0], &r = buf[1], &p = buf[2], &v = buf[3], &s_ = buf[4], &t = buf[5],
+         &p_ = buf[6], &s2 = buf[7];
+    std::vector<double> rho0(NV), res(NV);
+    // 1-2: r0 = b - A x; rho0 = (r0, r0); p = r = r0 (rho = rho0)
+    if (x.zero)
+        ops::group1_zero(n, b.p<double>(), r0.p<double>(), p.p<double>(), r.p<double>(), SC, NV, s);
+    else
+        ops::group1(*A, x.p<double>(), b.p<double>(), r0.p<double>(), p.p<double>(),
+                    r.p<double>(), SC, NV, s);
+    r0.zero = p.zero = r.zero = false;
+    read_scalars(SC + k::SC_RHO0 * k::SC_STRIDE, rho0.data(), NV);
+    if (check(rho0.data(), rho0.data(), iconv)) return;
+    const bool has_M = (M != nullptr);
+    do {
+        ++st.iters;
+        DVec *pa = &p, *sa = &s_;
+        if (has_M) {
+            apply_M(p_, p);
+            pa = &p_;
+        }
+        // v = A p_; alpha = rho / (v, r0)
+        ops::spmv_dot_alpha(*A, pa->p<double>(), v.p<double>(), r0.p<double>(), SC, NV, s);
+        v.zero = false;
+        // s = r - alpha v
+        ops::s_update(n, s_.p<double>(), r.p<double>(), v.p<double>(), SC, NV, s);
+        s_.zero = false;
+        if (has_M) {
+            apply_M(s2, s_);
+            sa = &s2;
+        }
+        // t = A s_; omega = (t,s)/(t,t); res = (s,s) - omega (t,s)
+        ops::spmv_dot3(*A, sa->p<double>(), t.p<double>(), s_.p<double>(), SC, NV, s);
+        t.zero = false;
+        read_scalars(SC + k::SC_RES * k::SC_STRIDE, res.data(), NV);
+        const bool done = check(res.data(), rho0.data(), iconv);
+        if (precond_form) {
+            if (done) {
+                ops::x_update(n, x.p<double>(), pa->p<double>(), sa->p<double>(), SC, NV, s);
+                x.zero = false;
+                return;
+            }
+            // x update fused with r = s - omega t; rho = (r, r0); beta
+            ops::group4(n, s_.p<double>(), t.p<double>(), r0.p<double>(), r.p<double>(),
+                        x.p<double>(), pa->p<double>(), sa->p<double>(), true, SC, NV, s);
+            x.zero = false;
+            ops::p_update(n, p.p<double>(), r.p<double>(), v.p<double>(), SC, NV, s);
+        } else {
+            if (done) {
+                ops::x_update(n, x.p<double>(), p.p<double>(), s_.p<double>(), SC, NV, s);
+                x.zero = false;
+                return;
+            }
+            ops::group4(n, s_.p<double>(), t.p<double>(), r0.p<double>(), r.p<double>(), nullptr,
+                        nullptr, nullptr, false, SC, NV, s);
+            ops::group5(n, x.p<double>(), p.p<double>(), s_.p<double>(), r.p<double>(),
+                        v.p<double>(), SC, NV, s);
+            x.zero = false;
+        }
+    } while (st.iters < cfg.max_iters);
+    XG_CUDA(cudaStreamSynchronize(s));
+}
+
+// ===========================================================================
+// construct_solver_hierarchy (solver.h:259-276, 481-500)
+// ===========================================================================
+void SolverHierarchy::build(const Params &P, const HCsr &hA_, const DCsr *A_, int nv) {
+    params = P;
+    hA = hA_;
+    A = A_;
+    NV = nv;
+    XG_REQUIRE(P.has("solver"), XAMG_ERR_INVALID_ARG, "parameters have no 'solver' list");
+    SolverCfg c = resolve_cfg(P.get("solver"), "solver");
+    const std::string &m = c.method;
+    mg = nullptr;
+    if (m == "MultiGrid") {
+        auto *g = new MultiGrid();
+        g->build(hA, A, P, "solver", nv);
+        mg = g;
+        root.reset(g);
+        return;
+    }
+    if (m == "MergedPBiCGStab" || m == "PBiCGStab" || m == "MergedBiCGStab" || m == "BiCGStab") {
+        auto *kr = new Krylov();
+        kr->cfg = c;
+        kr->role = "solver";
+        kr->NV = nv;
+        kr->A = A;
+        kr->n = hA.nrows;
+        kr->precond_form = (m != "MergedBiCGStab");
+        kr->setup();
+        const bool wants_M = (m == "MergedPBiCGStab" || m == "PBiCGStab");
+        if (wants_M && P.has("preconditioner")) {
+            SolverCfg pc = resolve_cfg(P.get("preconditioner"), "preconditioner");
+            if (pc.method == "MultiGrid") {
+                auto *g = new MultiGrid();
+                g->build(hA, A, P, "preconditioner", nv);
+                mg = g;
+                kr->M.reset(g);
+            } else {
+                kr->M = make_smoother(pc, "preconditioner", *A, hA, false, nv, 0, 0);
+                if (pc.method == "Chebyshev") {
+                    double mn, mx;
+                    estimate_eigs(hA, 10, pc.gpu_seed, mn, mx);
+                    auto *ch = dynamic_cast<Chebyshev<double> *>(kr->M.get());
+                    if (ch) {
+                        ch->min_eig = mn;
+                        ch->max_eig = mx;
+                    }
+                }
+            }
+        } else if (wants_M) {
+            // no preconditioner list: Identity (p_ = p), as XAMG's default
+            SolverCfg ic;
+            ic.method = "Identity";
+            kr->M = make_smoother(ic, "preconditioner", *A, hA, false, nv, 0, 0);
+        }
+        root.reset(kr);
+        return;
+    }
+    if (m == "Jacobi" || m == "HSGS" || m == "Chebyshev" || m == "Direct" || m == "Identity") {
+        double mn = 0, mx = 0;
+        if (m == "Chebyshev") estimate_eigs(hA, 10, c.gpu_seed, mn, mx);
+        root = make_smoother(c, "solver", *A, hA, false, nv, mn, mx);
+        return;
+    }
+    throw Error(XAMG_ERR_UNSUPPORTED, "solver method not implemented: " + m);
+}
+
+void SolverHierarchy::solve(DVec &x, DVec &b) {
+    std::vector<double> ones(NV, 1.0);
+    root->solve(x, b, ones);
+    XG_CUDA(cudaStreamSynchronize(ctx().stream));
+}
+
+}  // namespace xg

@@ -1,0 +1,95 @@
+// Solver objects of the B200 solve phase: the XAMG method set (solver.h:417-441)
+// on device data. Each class restates the control flow of the reference's
+// solvers/detail/*.inl, keeps XAMG's zero-flag short-circuits (they decide
+// which kernels run) and replaces each blas/blas2 call sequence with fused
+// kernels that write the same values.
+#pragma once
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "amg.h"
+#include "device.h"
+#include "params.h"
+
+namespace xg {
+
+struct Stats {
+    std::vector<int> conv;
+    std::vector<double> abs_res, rel_res;
+    int iters = 0;
+};
+
+struct SolverBase {
+    SolverCfg cfg;
+    std::string role;
+    int NV = 1;
+    bool f32 = false;
+    const DCsr *A = nullptr;
+    uint64_t n = 0;
+    Stats st;
+    std::vector<DVec> buf;
+    virtual ~SolverBase() {}
+    virtual void setup() {}
+    // conv: NV entries, 1 = still active, 0 = converged (the "iconv" vector)
+    virtual void solve(DVec &x, DVec &b, const std::vector<double> &conv) = 0;
+    void reset_stats();
+    void alloc_buffers(int count);
+};
+
+struct MgLevel {
+    bool f32 = false;       // working precision of A and the smoothers
+    bool tf32 = false;      // precision of R and P
+    DCsr A, R, P;
+    DVec temp, bH, xH;
+    double min_eig = 0, max_eig = 0;
+    HCsr hA;                // host copy (for the smoothers' setup)
+};
+
+std::unique_ptr<SolverBase> make_smoother(const SolverCfg &cfg, const std::string &role,
+                                          const DCsr &A, const HCsr &hA, bool f32, int nv,
+                                          double min_eig, double max_eig);
+
+class MultiGrid : public SolverBase {
+  public:
+    std::vector<MgLevel> L;
+    std::vector<std::unique_ptr<SolverBase>> pre, post;
+    std::unique_ptr<SolverBase> coarse;
+    Hierarchy H;  // kept for export
+    void build(const HCsr &A0, const DCsr *A0dev, const Params &P, const std::string &role,
+               int nv);
+    void solve(DVec &x, DVec &b, const std::vector<double> &conv) override;
+
+  private:
+    void cycle(int level, DVec &x, DVec &b, int cyc, const std::vector<double> &iconv);
+};
+
+class Krylov : public SolverBase {
+  public:
+    bool precond_form = true;  // (P)BiCGStab structure; false: MergedBiCGStab
+    std::unique_ptr<SolverBase> M;
+    DevBuf sc;                 // scalar block (kernels.cuh Sc)
+    void setup() override;
+    void solve(DVec &x, DVec &b, const std::vector<double> &conv) override;
+
+  private:
+    bool check(const double *res, const double *res0, std::vector<double> &iconv);
+    void apply_M(DVec &out, DVec &in);
+    void upload_iconv(const std::vector<double> &iconv);
+};
+
+// The solver hierarchy of XAMG_solver_create* (construct_solver_hierarchy,
+// solver.h:481-500): outer method, optional preconditioner.
+struct SolverHierarchy {
+    Params params;
+    HCsr hA;            // host copy of the fine matrix
+    const DCsr *A = nullptr;
+    int NV = 1;
+    std::unique_ptr<SolverBase> root;
+    MultiGrid *mg = nullptr;  // the multigrid object, if any
+    void build(const Params &P, const HCsr &hA_, const DCsr *A_, int nv);
+    void solve(DVec &x, DVec &b);
+};
+
+}  // namespace xg

@@ -1,0 +1,207 @@
+"""Whole solves through the public XAMG C API on the GPU, checked against the
+oracle. With the oracle replaying the kernels' fixed reduction order (mode 1)
+the GPU solution, iteration count and residuals must be identical bit for
+bit; against XAMG's own sequential order (mode 0) they must agree to 1e-6
+relative with both true residuals at the tolerance."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+pytestmark = pytest.mark.gpu
+
+MG_BASE = {"mg_agg_num_levels": 0, "mg_strength_threshold": 0.25, "mg_coarsening_type": 8,
+           "mg_interpolation_type": 6, "mg_coarse_matrix_size": 60, "max_iters": 1}
+
+
+def gpu_solve(xamg, row, col, val, nv, params, b, x0=None, overrides=None):
+    M = xamg.Matrix(row, col, val)
+    X = xamg.Vector(M.n, nv, M.part)
+    B = xamg.Vector(M.n, nv, M.part)
+    B.upload(b)
+    if x0 is None:
+        X.set(0.0)
+    else:
+        X.upload(x0)
+    P = xamg.Params(params, overrides=overrides)
+    S = xamg.Solver(M, P, X, B)
+    S.solve()
+    return X.download(), S.stats(), S
+
+
+def oracle_solve(oracle, S_gpu, row, col, val, nv, params, b, mode, x0=None, hsgs_rows=32):
+    sysm = oracle.System(nv)
+    sysm.set_params(params)
+    sysm.hsgs_cores(-hsgs_rows)
+    mg = "MultiGrid" in (params.get("solver", {}).get("method"),
+                         params.get("preconditioner", {}).get("method"))
+    if mg:
+        for lv in S_gpu.hierarchy():
+            sysm.add_level(*lv["A"], lv["min_eig"], lv["max_eig"])
+            if lv["P"] is not None:
+                sysm.add_interp(*lv["P"])
+    else:
+        sysm.add_level(row, col, val)
+    sysm.setup()
+    oracle.set_reduction(mode)
+    try:
+        x, st = sysm.solve(b, x0)
+    finally:
+        oracle.set_reduction(0)
+    return x, st, sysm
+
+
+def true_rel_res(row, col, val, x, b, nv):
+    A = sp.csr_matrix((val.copy(), col.copy(), row.copy()))
+    X, Bm = x.reshape(-1, nv), b.reshape(-1, nv)
+    return np.linalg.norm(Bm - A @ X, axis=0) / np.linalg.norm(Bm, axis=0)
+
+
+def check(xamg, oracle, row, col, val, nv, params, seed=0, tol=1e-8, overrides=None,
+          hsgs_rows=32):
+    n = len(row) - 1
+    b = np.random.default_rng(seed).uniform(-1, 1, n * nv)
+    xg, sg, S = gpu_solve(xamg, row, col, val, nv, params, b, overrides=overrides)
+    # bit-exact against the replay of the kernels' order
+    xo, so, _ = oracle_solve(oracle, S, row, col, val, nv, params, b, 1, hsgs_rows=hsgs_rows)
+    assert sg["iters"] == so["iters"]
+    assert sg["conv"].tolist() == so["conv"].tolist()
+    assert sg["rel_res"].tobytes() == so["rel_res"].tobytes()
+    assert xg.tobytes() == xo.tobytes(), np.abs(xg - xo).max()
+    # against XAMG's sequential order
+    xs, ss, _ = oracle_solve(oracle, S, row, col, val, nv, params, b, 0, hsgs_rows=hsgs_rows)
+    assert all(sg["conv"]) and all(ss["conv"])
+    rg = true_rel_res(row, col, val, xg, b, nv)
+    rs = true_rel_res(row, col, val, xs, b, nv)
+    assert rg.max() <= 2 * tol and rs.max() <= 2 * tol, (rg, rs)
+    dx = np.linalg.norm((xg - xs).reshape(-1, nv), axis=0) / np.linalg.norm(xs.reshape(-1, nv),
+                                                                             axis=0)
+    assert dx.max() <= 1e-6, dx
+    return sg, S
+
+
+def test_config1_merged_pbicgstab_jacobi(gpu, oracle):
+    """32^3 Poisson, nv = 1, MergedPBiCGStab + Jacobi, FP64, 1e-8."""
+    row, col, val = gpu.generate_cube(32, 32, 32)
+    params = {"solver": {"method": "MergedPBiCGStab", "max_iters": 1000, "rel_tolerance": 1e-8,
+                         "abs_tolerance": 0},
+              "preconditioner": {"method": "Jacobi"}}
+    st, S = check(gpu, oracle, row, col, val, 1, params)
+    assert 30 < st["iters"] < 80
+    # XAMG narrowing: 32768 columns -> 2-byte column indices on the device
+    assert S.level_info(0, 0)["col_bytes"] == 2
+
+
+@pytest.mark.parametrize("method", ["PBiCGStab", "BiCGStab", "MergedBiCGStab"])
+@pytest.mark.parametrize("nv", [2, 8])
+def test_krylov_variants(gpu, oracle, method, nv):
+    row, col, val = gpu.generate_cube(14, 13, 12)
+    params = {"solver": {"method": method, "max_iters": 500, "rel_tolerance": 1e-9,
+                         "abs_tolerance": 0}}
+    if method == "PBiCGStab":
+        params["preconditioner"] = {"method": "Jacobi", "max_iters": 3}
+    check(gpu, oracle, row, col, val, nv, params, seed=nv, tol=1e-9)
+
+
+@pytest.mark.parametrize("smoother,reduced", [("Jacobi", 0), ("Chebyshev", 0), ("HSGS", 0),
+                                              ("Chebyshev", 1), ("HSGS", 1), ("Jacobi", 1)])
+def test_amg_preconditioner(gpu, oracle, smoother, reduced):
+    row, col, val = gpu.generate_diffusion(7, 18, 17, 16, 1.0, 1.0, 0)
+    nv = 4
+    sm = {"method": smoother}
+    if smoother == "Chebyshev":
+        sm["polynomial_order"] = 2
+    if smoother == "HSGS":
+        sm["max_iters"] = 1
+    params = {"solver": {"method": "MergedPBiCGStab", "max_iters": 300, "rel_tolerance": 1e-8,
+                         "abs_tolerance": 0},
+              "preconditioner": dict(MG_BASE, method="MultiGrid", mg_reduced_precision=reduced),
+              "pre_smoother": sm, "post_smoother": dict(sm), "coarse_grid_solver": {"method": "Direct"}}
+    st, S = check(gpu, oracle, row, col, val, nv, params, seed=5)
+    assert S.nlevels() >= 3
+    assert st["iters"] < 60
+
+
+def test_uploaded_levels_match_oracle_narrowing(gpu, oracle):
+    """Every uploaded level matrix equals, bit for bit, what XAMG's parse of the
+    same hierarchy produces: values converted to float when reduced, columns
+    narrowed to define_int_type(ncols), R = transpose(P)."""
+    row, col, val = gpu.generate_diffusion(27, 12, 12, 12, 1.0, 1.0, 1)
+    nv = 2
+    params = {"solver": {"method": "PBiCGStab", "max_iters": 100},
+              "preconditioner": dict(MG_BASE, method="MultiGrid", mg_reduced_precision=1),
+              "pre_smoother": {"method": "Chebyshev"}, "post_smoother": {"method": "Chebyshev"}}
+    b = np.random.default_rng(0).uniform(-1, 1, (len(row) - 1) * nv)
+    _, _, S = gpu_solve(gpu, row, col, val, nv, params, b)
+    _, _, sysm = oracle_solve(oracle, S, row, col, val, nv, params, b, 1)
+    nl = S.nlevels()
+    assert nl >= 3
+    for l in range(nl):
+        for which in ((0, 1, 2) if l + 1 < nl else (0,)):
+            r, c, v, info = S.level_download(l, which)
+            orow, ocol, oval, oncols = sysm.level_matrix(l, which)
+            assert info["col_bytes"] == {0: 1, 1: 2, 2: 4}[oracle.define_int_type(info["ncols"])]
+            assert info["hash"] == oracle.encode_hash(info["nnz"], info["ncols"], info["nrows"],
+                                                      info["ncols"], reduced=info["f32"])
+            assert r.tobytes() == orow.tobytes()
+            assert c.astype(np.uint32).tobytes() == ocol.tobytes()
+            assert v.dtype == oval.dtype and v.tobytes() == oval.tobytes()
+
+
+def test_multigrid_as_solver(gpu, oracle):
+    row, col, val = gpu.generate_diffusion(7, 16, 16, 16, 1.0, 1.0, 2)
+    params = {"solver": dict(MG_BASE, method="MultiGrid", max_iters=100, rel_tolerance=1e-8,
+                             abs_tolerance=0),
+              "pre_smoother": {"method": "Jacobi"}, "post_smoother": {"method": "Jacobi"}}
+    check(gpu, oracle, row, col, val, 2, params, seed=9)
+
+
+def test_jacobi_as_solver(gpu, oracle):
+    row, col, val = gpu.generate_cube(8, 8, 8)
+    params = {"solver": {"method": "Jacobi", "max_iters": 2000, "rel_tolerance": 1e-6,
+                         "abs_tolerance": 0}}
+    check(gpu, oracle, row, col, val, 1, params, tol=1e-6)
+
+
+def test_zero_rhs_converges_at_once(gpu):
+    row, col, val = gpu.generate_cube(6, 6, 6)
+    params = {"solver": {"method": "MergedPBiCGStab"}, "preconditioner": {"method": "Jacobi"}}
+    x, st, S = gpu_solve(gpu, row, col, val, 4, params, np.zeros(216 * 4))
+    assert st["iters"] == 0 and all(st["conv"])
+    assert not x.any()
+
+
+def test_renew_params_and_solve2(gpu):
+    row, col, val = gpu.generate_cube(12, 12, 12)
+    n, nv = len(row) - 1, 2
+    params = {"solver": {"method": "PBiCGStab", "max_iters": 500, "rel_tolerance": 1e-4,
+                         "abs_tolerance": 0},
+              "preconditioner": {"method": "Jacobi"}}
+    b = np.random.default_rng(0).uniform(-1, 1, n * nv)
+    x, st1, S = gpu_solve(gpu, row, col, val, nv, params, b)
+    P2 = gpu.Params({"solver": {"rel_tolerance": 1e-10}}, set_default=False)
+    S.renew(P2)
+    M = gpu.Matrix(row, col, val)
+    X = gpu.Vector(n, nv)
+    B = gpu.Vector(n, nv)
+    X.set(0.0)
+    B.upload(b)
+    S.solve(X, B)
+    st2 = S.stats()
+    assert st2["iters"] > st1["iters"]
+    assert true_rel_res(row, col, val, X.download(), b, nv).max() < 1e-9
+    assert S.convergence_info().tolist() == [1, 1]
+
+
+def test_nv_mismatch_is_an_error(gpu):
+    row, col, val = gpu.generate_cube(4, 4, 4)
+    M = gpu.Matrix(row, col, val)
+    X = gpu.Vector(64, 2)
+    B = gpu.Vector(64, 2)
+    X.set(0.0)
+    B.set(1.0)
+    S = gpu.Solver(M, gpu.Params({"solver": {"method": "BiCGStab"}}), X, B)
+    with pytest.raises(gpu.XamgError) as e:
+        gpu.call("XAMG_solver_solve1", 4, S.h)
+    assert e.value.code == -3
+    with pytest.raises(gpu.XamgError):
+        gpu.call("XAMG_vector_alloc_d", 10, 3, X.h)
