@@ -123,7 +123,8 @@ PValue pv_f(float f) {
 struct BorrowedCsr {
     DCsr d;
     explicit BorrowedCsr(const XAMG_b200_csr *A) {
-        XG_REQUIRE(A && A->row && A->col && A->val, XAMG_ERR_INVALID_ARG, "null CSR descriptor");
+        XG_REQUIRE(A && A->row && ((A->col && A->val) || A->nnz == 0), XAMG_ERR_INVALID_ARG,
+                   "null CSR descriptor");
         XG_REQUIRE(A->col_bytes == 1 || A->col_bytes == 2 || A->col_bytes == 4,
                    XAMG_ERR_INVALID_ARG, "col_bytes must be 1, 2 or 4");
         d.nrows = A->nrows;

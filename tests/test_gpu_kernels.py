@@ -141,7 +141,8 @@ def test_merged_groups_canonical(gpu, oracle, nv):
         assert rho.tobytes() == o_rho.tobytes()
         # group2
         phi, psi, th = np.zeros(nv), np.zeros(nv), np.zeros(nv)
-        gpu.call("XAMG_b200_group2", n, nv, torch_dev(t).data_ptr(), torch_dev(s).data_ptr(),
+        td, sd, r0dd = torch_dev(t), torch_dev(s), torch_dev(r0)  # kept alive across the calls
+        gpu.call("XAMG_b200_group2", n, nv, td.data_ptr(), sd.data_ptr(),
                  phi.ctypes.data_as(C.c_void_p), psi.ctypes.data_as(C.c_void_p),
                  th.ctypes.data_as(C.c_void_p), None)
         o = [np.zeros(nv) for _ in range(3)]
@@ -151,8 +152,8 @@ def test_merged_groups_canonical(gpu, oracle, nv):
         # group4
         rd = torch_dev(np.zeros(n * nv))
         rho4 = np.zeros(nv)
-        gpu.call("XAMG_b200_group4", n, nv, torch_dev(s).data_ptr(), torch_dev(t).data_ptr(),
-                 torch_dev(r0).data_ptr(), rd.data_ptr(), om.ctypes.data_as(C.c_void_p),
+        gpu.call("XAMG_b200_group4", n, nv, sd.data_ptr(), td.data_ptr(),
+                 r0dd.data_ptr(), rd.data_ptr(), om.ctypes.data_as(C.c_void_p),
                  rho4.ctypes.data_as(C.c_void_p), None)
         o_r, o_rho = np.zeros(n * nv), np.zeros(nv)
         oracle.lib().or_group4(n, nv, s, t, r0, o_r, om, o_rho)
@@ -173,8 +174,9 @@ def test_spmv_dot_fused(gpu, oracle, nv):
     A, keep = dev_csr(gpu, row, col, val, n, 2, False)
     vd = torch_dev(np.zeros(n * nv))
     dot = np.zeros(nv)
-    gpu.call("XAMG_b200_spmv_dot", C.byref(A), torch_dev(x).data_ptr(), vd.data_ptr(),
-             torch_dev(z).data_ptr(), dot.ctypes.data_as(C.c_void_p), nv, None)
+    xd, zd = torch_dev(x), torch_dev(z)  # kept alive until the kernel has run
+    gpu.call("XAMG_b200_spmv_dot", C.byref(A), xd.data_ptr(), vd.data_ptr(),
+             zd.data_ptr(), dot.ctypes.data_as(C.c_void_p), nv, None)
     v = oracle.csr_ax_y(row, col, val, x, nv, ncols=n)
     assert vd.cpu().numpy().tobytes() == v.tobytes()
     oracle.set_reduction(1)

@@ -70,9 +70,11 @@ def check(xamg, oracle, row, col, val, nv, params, seed=0, tol=1e-8, overrides=N
     # against XAMG's sequential order
     xs, ss, _ = oracle_solve(oracle, S, row, col, val, nv, params, b, 0, hsgs_rows=hsgs_rows)
     assert all(sg["conv"]) and all(ss["conv"])
+    # the convergence test uses the recursive residual (res = theta - omega*phi,
+    # merged_bicgstab.inl:170-171); the true residual may drift a little above it
     rg = true_rel_res(row, col, val, xg, b, nv)
     rs = true_rel_res(row, col, val, xs, b, nv)
-    assert rg.max() <= 2 * tol and rs.max() <= 2 * tol, (rg, rs)
+    assert rg.max() <= 10 * tol and rs.max() <= 10 * tol, (rg, rs)
     dx = np.linalg.norm((xg - xs).reshape(-1, nv), axis=0) / np.linalg.norm(xs.reshape(-1, nv),
                                                                              axis=0)
     assert dx.max() <= 1e-6, dx
