@@ -40,7 +40,10 @@ int XAMG_b200_last_error(char *buf, size_t len);
 int XAMG_b200_build_info(char *buf, size_t len);
 
 /* A CSR block resident in device memory, with XAMG's narrowed column type
- * (col_bytes = 1, 2 or 4; csr_matrix.h:47-86 with I2 in {u8,u16,u32}).
+ * (col_bytes = 1, 2 or 4; csr_matrix.h:47-86 with I2 in {u8,u16,u32}), or
+ * col_bytes = -2: signed 16-bit offsets col - row, a form with no
+ * counterpart in the reference, used for square matrices whose entries all
+ * lie within 32767 of the diagonal (parameter gpu_index_compress = 2).
  * Row pointers are 32-bit. Values are double (val_f32 = 0) or float. */
 typedef struct {
     uint64_t nrows, ncols, nnz;

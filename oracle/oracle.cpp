@@ -1532,6 +1532,22 @@ static void solve_mg(Solver &S, Vec &x, Vec &b, const Vec &conv) {
         if (converged<double>(S, rho0, rho0, iconv)) return;
     }
     const bool reduced = (*S.levels)[1].reduced;
+    if ((*S.levels)[0].reduced) {
+        // B200 extension (gpu_precond_f32 = 1, preconditioner only): every
+        // level in float, the input converted on entry and the result on exit
+        const uint64_t n = (*S.levels)[0].A.nrows;
+        Vec b32 = make_vec<float>(n, NV), x32 = make_vec<float>(n, NV);
+        Vec ic32 = make_vec<float>(1, NV);
+        convert_vec<double>(b, b32);
+        convert_vec<double>(x, x32);
+        convert_vec<double>(iconv, ic32);
+        do {
+            ++it;
+            mg_cycle<float, float>(S, x32, b32, 0, S.sp.mg_cycle, ic32);
+        } while (it < S.sp.max_iters);
+        convert_vec<float>(x32, x);
+        return;
+    }
     do {
         ++it;
         if (reduced)
@@ -1788,10 +1804,17 @@ static int setup(System &sys) {
     const bool mg_solver = (sol == "MultiGrid");
     const bool mg_prec = (pre == "MultiGrid");
     const std::string mg_role = mg_solver ? "solver" : "preconditioner";
-    bool reduced = false;
+    bool reduced = false, full32 = false;
     if (mg_solver || mg_prec) {
         std::string v = sys.P.get(mg_role, "mg_reduced_precision");
         reduced = !v.empty() && std::stol(v) != 0;
+        // B200 extension: gpu_precond_f32 = 1 puts the finest level of the
+        // multigrid preconditioner in float too (0: none, unset: XAMG's rule)
+        std::string g = sys.P.get(mg_role, "gpu_precond_f32");
+        if (!g.empty()) {
+            reduced = std::stol(g) != 0;
+            full32 = mg_prec && std::stol(g) == 1;
+        }
     }
     // hierarchy parse: hypre_base.inl:337-403 (A_l, eigenvalue estimates,
     // P_l and R_l = transpose(P_l), converted to float when reduced)
@@ -1799,7 +1822,7 @@ static int setup(System &sys) {
     sys.levels.assign(L, Level());
     for (size_t l = 0; l < L; ++l) {
         Level &lv = sys.levels[l];
-        lv.reduced = (l >= 1) && reduced;
+        lv.reduced = (l >= 1 || full32) && reduced;
         lv.A = lv.reduced ? to_f32(sys.A64[l]) : sys.A64[l];
         lv.min_eig = sys.min_eig[l];
         lv.max_eig = sys.max_eig[l];
@@ -1850,13 +1873,13 @@ static int setup(System &sys) {
     if (mg_solver) {
         sys.root = build_mg("solver");
     } else {
-        sys.root = make_basic(sys, "solver", -1, sys.levels[0].A, false, sys.levels[0].min_eig,
+        sys.root = make_basic(sys, "solver", -1, sys.A64[0], false, sys.levels[0].min_eig,
                               sys.levels[0].max_eig);
         if (sys.P.has("preconditioner")) {
             if (mg_prec)
                 sys.root->precond = build_mg("preconditioner");
             else
-                sys.root->precond = make_basic(sys, "preconditioner", -1, sys.levels[0].A, false,
+                sys.root->precond = make_basic(sys, "preconditioner", -1, sys.A64[0], false,
                                                sys.levels[0].min_eig, sys.levels[0].max_eig);
         }
     }

@@ -41,10 +41,11 @@ struct CsrObj {
 struct MatObj {
     HCsr h;
     bool constructed = false;
+    HierCache hcache;  // host multigrid hierarchies built for this matrix
     // device copies keyed by the narrowing switch
     std::map<int, std::unique_ptr<DCsr>> dev;
-    const DCsr *device(bool narrow) {
-        auto &p = dev[narrow ? 1 : 0];
+    const DCsr *device(int narrow) {
+        auto &p = dev[narrow];
         if (!p) {
             p.reset(new DCsr());
             upload_csr(h, *p, false, narrow, ctx().stream);
@@ -125,8 +126,9 @@ struct BorrowedCsr {
     explicit BorrowedCsr(const XAMG_b200_csr *A) {
         XG_REQUIRE(A && A->row && ((A->col && A->val) || A->nnz == 0), XAMG_ERR_INVALID_ARG,
                    "null CSR descriptor");
-        XG_REQUIRE(A->col_bytes == 1 || A->col_bytes == 2 || A->col_bytes == 4,
-                   XAMG_ERR_INVALID_ARG, "col_bytes must be 1, 2 or 4");
+        XG_REQUIRE(A->col_bytes == 1 || A->col_bytes == 2 || A->col_bytes == 4 ||
+                       A->col_bytes == -2,
+                   XAMG_ERR_INVALID_ARG, "col_bytes must be 1, 2, 4 or -2");
         d.nrows = A->nrows;
         d.ncols = A->ncols;
         d.nnz = A->nnz;
@@ -486,6 +488,7 @@ int XAMG_matrix_construct(XAMG_csr_matrix_id cid, XAMG_matrix_id mid) {
                    "the single-GPU solve phase needs a square matrix on one rank");
         m.h = c.h;
         m.dev.clear();
+        m.hcache.clear();
         m.constructed = true;
     });
 }
@@ -500,10 +503,10 @@ static void build_solver(SolverObj &so, const Params &P, int nv) {
     MatObj &m = get(g_mats, so.mid, "matrix");
     XG_REQUIRE(m.constructed, XAMG_ERR_INVALID_ARG, "matrix not constructed");
     SolverCfg c = resolve_cfg(P.get("solver"), "solver");
-    const bool narrow = c.gpu_index_compress != 0;
+    const int narrow = c.gpu_index_compress;
     const DCsr *A = m.device(narrow);
     so.sh.reset(new SolverHierarchy());
-    so.sh->build(P, m.h, A, nv);
+    so.sh->build(P, m.h, A, nv, &m.hcache);
     so.nv = nv;
 }
 
@@ -829,10 +832,10 @@ int XAMG_b200_solver_hierarchy_export(size_t sid, int level, int which, uint32_t
             XG_REQUIRE(level == 0 && which == 0, XAMG_ERR_INVALID_ARG, "no multigrid hierarchy");
             h = &so.sh->hA;
         } else {
-            XG_REQUIRE(level >= 0 && level < (int)mg->H.lv.size(), XAMG_ERR_INVALID_ARG,
+            XG_REQUIRE(level >= 0 && level < (int)mg->H->lv.size(), XAMG_ERR_INVALID_ARG,
                        "bad level");
             XG_REQUIRE(which == 0 || which == 2, XAMG_ERR_INVALID_ARG, "which must be 0 or 2");
-            h = which == 0 ? &mg->H.lv[level].A : &mg->H.lv[level].P;
+            h = which == 0 ? &mg->H->lv[level].A : &mg->H->lv[level].P;
         }
         if (row) std::memcpy(row, h->row.data(), h->row.size() * sizeof(uint32_t));
         if (col) std::memcpy(col, h->col.data(), h->col.size() * sizeof(uint32_t));

@@ -124,7 +124,11 @@ struct DCsr {
 // Upload `h` narrowed per XAMG's rule (define_int_type on ncols for the
 // column width; the I1 row-pointer width only enters the hash since row
 // pointers stay 32-bit on the device). reduced_prec stores float values.
-void upload_csr(const HCsr &h, DCsr &d, bool f32, bool narrow, cudaStream_t s);
+// narrow: 0 keeps 32-bit columns; 1 applies XAMG's rule; 2 additionally
+// stores signed 16-bit offsets col - row (col_bytes = -2) for square
+// matrices whose columns need more than 16 bits but whose entries all lie
+// within 32767 of the diagonal.
+void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s);
 void download_csr(const DCsr &d, uint32_t *row, void *col, void *val);
 
 template <typename T>

@@ -28,6 +28,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 namespace xg {
 namespace k {
@@ -159,27 +160,83 @@ struct CsrArgs {
     uint64_t n;
 };
 
+// Shared-memory staging: a tile's entries [row[r0], row[r0+R]) are copied into
+// shared memory by all 256 threads with coalesced loads (many loads in flight
+// per thread), then every thread walks its own row from shared memory. Tiles
+// with more entries than the staging capacity read global memory directly.
+template <typename F>
+struct StageCap {
+    static constexpr int value = sizeof(F) == 8 ? 2048 : 3072;  // 24 KB per block
+};
+
+// Column index of entry j: narrowed absolute index (I unsigned) or, for
+// I = int16_t, a signed offset from the row index (the 2-byte relative form
+// used where every |col - row| < 32768).
+template <typename I>
+__device__ __forceinline__ uint64_t col_of(const I *col, uint64_t j, uint64_t i) {
+    if constexpr (std::is_same<I, int16_t>::value)
+        return (uint64_t)((int64_t)i + (int64_t)__ldg(&col[j]));
+    else
+        return (uint64_t)__ldg(&col[j]);
+}
+
 template <typename F, typename FX, typename I, int NV, int NRED, class Epi>
 __global__ void __launch_bounds__(CT)
     k_spmv(CsrArgs<F> A, const FX *__restrict__ x, Epi epi, RedArgs ra) {
     constexpr int R = CT / NV;
+    constexpr int CAP = StageCap<F>::value;
+    __shared__ F s_val[CAP];
+    __shared__ uint32_t s_col[CAP];
     const int rt = threadIdx.x / NV, k = threadIdx.x % NV;
     const uint32_t *__restrict__ row = A.row;
     const I *__restrict__ col = (const I *)A.col;
     const F *__restrict__ val = A.val;
-    const uint64_t ntiles = (A.n + R - 1) / R;
+    const uint64_t n = A.n;
+    const uint64_t ntiles = (n + R - 1) / R;
     F acc[NRED > 0 ? NRED : 1];
 #pragma unroll
     for (int r = 0; r < (NRED > 0 ? NRED : 1); ++r) acc[r] = F(0);
     for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const uint64_t i = tile * R + rt;
-        if (i < A.n) {
+        const uint64_t r0 = tile * R;
+        const uint64_t r1 = r0 + R < n ? r0 + R : n;
+        const uint32_t tj0 = __ldg(&row[r0]), tj1 = __ldg(&row[r1]);
+        const uint32_t cnt = tj1 - tj0;
+        const bool staged = cnt <= (uint32_t)CAP;
+        __syncthreads();  // the previous tile's readers are done with the buffers
+        if (staged) {
+            // rows of this tile own [tj0, tj1); the row index of entry e is only
+            // needed for the relative form, found by the owning thread below
+#pragma unroll 4
+            for (uint32_t e = threadIdx.x; e < cnt; e += CT) {
+                if constexpr (std::is_same<I, int16_t>::value)
+                    s_col[e] = (uint32_t)(int32_t)__ldg(&col[tj0 + e]);
+                else
+                    s_col[e] = (uint32_t)__ldg(&col[tj0 + e]);
+                s_val[e] = __ldg(&val[tj0 + e]);
+            }
+            __syncthreads();
+        }
+        const uint64_t i = r0 + rt;
+        if (i < n) {
             F y = epi.init(i, k);
             const uint32_t j0 = __ldg(&row[i]), j1 = __ldg(&row[i + 1]);
-            for (uint32_t j = j0; j < j1; ++j) {
-                const uint64_t c = (uint64_t)__ldg(&col[j]);
-                const F xv = (F)__ldg(&x[c * NV + k]);
-                y = add(y, mul(xv, __ldg(&val[j])));
+            if (staged) {
+                const uint32_t a = j0 - tj0, b = j1 - tj0;
+#pragma unroll 4
+                for (uint32_t j = a; j < b; ++j) {
+                    uint64_t c;
+                    if constexpr (std::is_same<I, int16_t>::value)
+                        c = (uint64_t)((int64_t)i + (int64_t)(int32_t)s_col[j]);
+                    else
+                        c = (uint64_t)s_col[j];
+                    const F xv = (F)__ldg(&x[c * NV + k]);
+                    y = add(y, mul(xv, s_val[j]));
+                }
+            } else {
+                for (uint32_t j = j0; j < j1; ++j) {
+                    const F xv = (F)__ldg(&x[col_of(col, j, i) * NV + k]);
+                    y = add(y, mul(xv, __ldg(&val[j])));
+                }
             }
             epi.store(i, k, y, acc);
         }

@@ -29,7 +29,8 @@ static void dispatch_col(int cb, Fn &&fn) {
     case 1: fn((uint8_t *)nullptr); break;
     case 2: fn((uint16_t *)nullptr); break;
     case 4: fn((uint32_t *)nullptr); break;
-    default: throw Error(XAMG_ERR_INVALID_ARG, "column width must be 1, 2 or 4 bytes");
+    case -2: fn((int16_t *)nullptr); break;
+    default: throw Error(XAMG_ERR_INVALID_ARG, "column width must be 1, 2, 4 or -2 bytes");
     }
 }
 

@@ -132,7 +132,7 @@ template void axpy_k<float>(float *, const float *, const double *, uint64_t, in
 // CSR upload with XAMG's narrowing (matrix_block::assemble, matrix.h:78-93:
 // hash from encode_hash, values converted to float when reduced).
 // ---------------------------------------------------------------------------
-void upload_csr(const HCsr &h, DCsr &d, bool f32, bool narrow, cudaStream_t s) {
+void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s) {
     d.nrows = h.nrows;
     d.ncols = h.ncols;
     d.nnz = h.nnz();
@@ -142,8 +142,27 @@ void upload_csr(const HCsr &h, DCsr &d, bool f32, bool narrow, cudaStream_t s) {
     d.col_bytes = narrow ? int_type_bytes(i2 > I32_TYPE ? I32_TYPE : i2) : 4;
     XG_REQUIRE(d.ncols <= UINT32_MAX && d.nnz <= UINT32_MAX, XAMG_ERR_UNSUPPORTED,
                "matrix exceeds 32-bit indexing");
+    if (narrow >= 2 && d.col_bytes == 4 && h.nrows == h.ncols) {
+        bool fits = true;
+        for (uint64_t i = 0; i < h.nrows && fits; ++i)
+            for (uint64_t j = h.row[i]; j < h.row[i + 1]; ++j) {
+                const int64_t off = (int64_t)h.col[j] - (int64_t)i;
+                if (off < -32767 || off > 32767) {
+                    fits = false;
+                    break;
+                }
+            }
+        if (fits) d.col_bytes = -2;
+    }
     upload(d.row, h.row, s);
-    if (d.col_bytes == 4) {
+    if (d.col_bytes == -2) {
+        std::vector<int16_t> c(h.col.size());
+        for (uint64_t i = 0; i < h.nrows; ++i)
+            for (uint64_t j = h.row[i]; j < h.row[i + 1]; ++j)
+                c[j] = (int16_t)((int64_t)h.col[j] - (int64_t)i);
+        upload(d.col, c, s);
+        XG_CUDA(cudaStreamSynchronize(s));
+    } else if (d.col_bytes == 4) {
         upload(d.col, h.col, s);
     } else if (d.col_bytes == 2) {
         std::vector<uint16_t> c(h.col.begin(), h.col.end());

@@ -229,8 +229,8 @@ struct Hsgs : public SolverBase {
             dg.row[i + 1] = (uint32_t)dg.col.size();
             od.row[i + 1] = (uint32_t)od.col.size();
         }
-        upload_csr(dg, Adiag, f32, cfg.gpu_index_compress != 0, S());
-        upload_csr(od, Aoff, f32, cfg.gpu_index_compress != 0, S());
+        upload_csr(dg, Adiag, f32, cfg.gpu_index_compress, S());
+        upload_csr(od, Aoff, f32, cfg.gpu_index_compress, S());
         upload(boff, off, S());
         if (f32)
             upload(d, inv_diag_f32(hA, false), S());
@@ -433,32 +433,49 @@ std::unique_ptr<SolverBase> make_smoother(const SolverCfg &cfg, const std::strin
 // ===========================================================================
 // MultiGrid (mg.inl:97-334)
 // ===========================================================================
+static std::string hierarchy_key(const SolverCfg &c) {
+    char buf[256];
+    snprintf(buf, sizeof(buf), "th=%.9g mrs=%.9g tf=%.9g pmax=%d ml=%d cs=%d ct=%d it=%d seed=%d",
+             (double)c.mg_strength_threshold, (double)c.mg_max_row_sum, (double)c.mg_trunc_factor,
+             c.mg_Pmax_elements, c.mg_max_levels, c.mg_coarse_matrix_size, c.mg_coarsening_type,
+             c.mg_interpolation_type, c.gpu_seed);
+    return buf;
+}
+
 void MultiGrid::build(const HCsr &A0, const DCsr *A0dev, const Params &P, const std::string &rl,
-                      int nv) {
+                      int nv, HierCache *cache) {
     role = rl;
     NV = nv;
     cfg = resolve_cfg(P.get(role), role);
     A = A0dev;
     n = A0.nrows;
     f32 = false;
-    H = build_hierarchy(A0, cfg);
-    const int nl = (int)H.lv.size();
+    const std::string key = hierarchy_key(cfg);
+    if (cache && cache->count(key)) {
+        H = (*cache)[key];
+    } else {
+        H = std::make_shared<const Hierarchy>(build_hierarchy(A0, cfg));
+        if (cache) (*cache)[key] = H;
+    }
+    const Hierarchy &HH = *H;
+    const int nl = (int)HH.lv.size();
     XG_REQUIRE(nl >= 2, XAMG_ERR_UNSUPPORTED, "multigrid hierarchy has fewer than 2 levels");
     const bool reduced = cfg.gpu_precond_f32 >= 0 ? cfg.gpu_precond_f32 != 0
                                                   : cfg.mg_reduced_precision != 0;
-    const bool narrow = cfg.gpu_index_compress != 0;
+    full32 = (cfg.gpu_precond_f32 == 1) && role == "preconditioner";
+    const int narrow = cfg.gpu_index_compress;
     L.clear();
     L.resize(nl);
     for (int l = 0; l < nl; ++l) {
         MgLevel &lv = L[l];
-        lv.f32 = (l >= 1) && reduced;
+        lv.f32 = (l >= 1 || full32) && reduced;
         lv.tf32 = reduced;
-        lv.min_eig = H.lv[l].min_eig;
-        lv.max_eig = H.lv[l].max_eig;
-        if (l >= 1) upload_csr(H.lv[l].A, lv.A, lv.f32, narrow, S());
+        lv.min_eig = HH.lv[l].min_eig;
+        lv.max_eig = HH.lv[l].max_eig;
+        if (l >= 1 || full32) upload_csr(HH.lv[l].A, lv.A, lv.f32, narrow, S());
         if (l + 1 < nl) {
             // R = P^T (hypre_base.inl:400-401, transpose.inl:31-108)
-            const HCsr &Ph = H.lv[l].P;
+            const HCsr &Ph = HH.lv[l].P;
             HCsr R;
             R.nrows = Ph.ncols;
             R.ncols = Ph.nrows;
@@ -479,9 +496,13 @@ void MultiGrid::build(const HCsr &A0, const DCsr *A0dev, const Params &P, const 
             upload_csr(Ph, lv.P, lv.tf32, narrow, S());
             upload_csr(R, lv.R, lv.tf32, narrow, S());
         }
-        const uint64_t nrow = H.lv[l].A.nrows;
+        const uint64_t nrow = HH.lv[l].A.nrows;
         if (l == 0) {
-            lv.temp.alloc(nrow, nv, false);
+            lv.temp.alloc(nrow, nv, lv.f32);
+            if (full32) {
+                b32.alloc(nrow, nv, true);
+                x32.alloc(nrow, nv, true);
+            }
         } else {
             lv.temp.alloc(nrow, nv, lv.f32);
             lv.bH.alloc(nrow, nv, lv.f32);
@@ -491,17 +512,17 @@ void MultiGrid::build(const HCsr &A0, const DCsr *A0dev, const Params &P, const 
     pre.clear();
     post.clear();
     for (int l = 0; l + 1 < nl; ++l) {
-        const DCsr &Al = (l == 0) ? *A0dev : L[l].A;
+        const DCsr &Al = (l == 0 && !full32) ? *A0dev : L[l].A;
         SolverCfg pc = resolve_cfg(P.get("pre_smoother", l), "pre_smoother");
         SolverCfg qc = resolve_cfg(P.get("post_smoother", l), "post_smoother");
         pc.gpu_index_compress = qc.gpu_index_compress = cfg.gpu_index_compress;
-        pre.push_back(make_smoother(pc, "pre_smoother", Al, H.lv[l].A, L[l].f32, nv,
+        pre.push_back(make_smoother(pc, "pre_smoother", Al, HH.lv[l].A, L[l].f32, nv,
                                     L[l].min_eig, L[l].max_eig));
-        post.push_back(make_smoother(qc, "post_smoother", Al, H.lv[l].A, L[l].f32, nv,
+        post.push_back(make_smoother(qc, "post_smoother", Al, HH.lv[l].A, L[l].f32, nv,
                                      L[l].min_eig, L[l].max_eig));
     }
     SolverCfg cc = resolve_cfg(P.get("coarse_grid_solver"), "coarse_grid_solver");
-    coarse = make_smoother(cc, "coarse_grid_solver", L[nl - 1].A, H.lv[nl - 1].A, L[nl - 1].f32,
+    coarse = make_smoother(cc, "coarse_grid_solver", L[nl - 1].A, HH.lv[nl - 1].A, L[nl - 1].f32,
                            nv, L[nl - 1].min_eig, L[nl - 1].max_eig);
     buf.resize(1);
     buf[0].alloc(n, nv, false);
@@ -511,7 +532,7 @@ void MultiGrid::build(const HCsr &A0, const DCsr *A0dev, const Params &P, const 
 // mg.inl:166-260
 void MultiGrid::cycle(int level, DVec &x, DVec &b, int cyc, const std::vector<double> &iconv) {
     MgLevel &lv = L[level];
-    const DCsr &Al = (level == 0) ? *A : lv.A;
+    const DCsr &Al = (level == 0 && !full32) ? *A : lv.A;
     const int nl = (int)L.size();
     MgLevel &nx = L[level + 1];
     DVec &temp = lv.temp, &bH = nx.bH, &xH = nx.xH;
@@ -581,6 +602,23 @@ void MultiGrid::solve(DVec &x, DVec &b, const std::vector<double> &conv) {
     reset_stats();
     std::vector<double> iconv = conv, rho0(NV), res(NV);
     DVec &r = buf[0];
+    if (full32) {
+        // preconditioner in float throughout: convert the input, cycle, convert
+        // the result back (zero flags carried across)
+        b32.zero = b.zero;
+        if (!b.zero) ops::convert<float, double>(b32.p<float>(), b.p<double>(), b.elems(), S());
+        x32.zero = x.zero;
+        if (!x.zero) ops::convert<float, double>(x32.p<float>(), x.p<double>(), x.elems(), S());
+        b32.init = x32.init = true;
+        do {
+            ++st.iters;
+            cycle(0, x32, b32, cfg.mg_cycle, iconv);
+        } while (st.iters < cfg.max_iters);
+        x.zero = x32.zero;
+        if (!x32.zero) ops::convert<double, float>(x.p<double>(), x32.p<float>(), x.elems(), S());
+        x.init = true;
+        return;
+    }
     if (cfg.convergence_check) {
         residual_norm<double>(*A, x, b, r, NV, rho0.data());
         if (host_converged(*this, rho0.data(), rho0.data(), iconv)) return;
@@ -702,7 +740,8 @@ void Krylov::solve(DVec &x, DVec &b, const std::vector<double> &conv) {
 // ===========================================================================
 // construct_solver_hierarchy (solver.h:259-276, 481-500)
 // ===========================================================================
-void SolverHierarchy::build(const Params &P, const HCsr &hA_, const DCsr *A_, int nv) {
+void SolverHierarchy::build(const Params &P, const HCsr &hA_, const DCsr *A_, int nv,
+                            HierCache *cache) {
     params = P;
     hA = hA_;
     A = A_;
@@ -713,7 +752,7 @@ void SolverHierarchy::build(const Params &P, const HCsr &hA_, const DCsr *A_, in
     mg = nullptr;
     if (m == "MultiGrid") {
         auto *g = new MultiGrid();
-        g->build(hA, A, P, "solver", nv);
+        g->build(hA, A, P, "solver", nv, cache);
         mg = g;
         root.reset(g);
         return;
@@ -732,7 +771,7 @@ void SolverHierarchy::build(const Params &P, const HCsr &hA_, const DCsr *A_, in
             SolverCfg pc = resolve_cfg(P.get("preconditioner"), "preconditioner");
             if (pc.method == "MultiGrid") {
                 auto *g = new MultiGrid();
-                g->build(hA, A, P, "preconditioner", nv);
+                g->build(hA, A, P, "preconditioner", nv, cache);
                 mg = g;
                 kr->M.reset(g);
             } else {

@@ -5,6 +5,7 @@
 // kernels that write the same values.
 #pragma once
 
+#include <map>
 #include <memory>
 #include <string>
 #include <vector>
@@ -51,14 +52,23 @@ std::unique_ptr<SolverBase> make_smoother(const SolverCfg &cfg, const std::strin
                                           const DCsr &A, const HCsr &hA, bool f32, int nv,
                                           double min_eig, double max_eig);
 
+// Host hierarchies already built for a matrix, keyed by the setup parameters
+// they depend on (the reference rebuilds the hierarchy for every solver; here
+// solvers that differ only in precision or smoothers share one build).
+using HierCache = std::map<std::string, std::shared_ptr<const Hierarchy>>;
+
 class MultiGrid : public SolverBase {
   public:
     std::vector<MgLevel> L;
     std::vector<std::unique_ptr<SolverBase>> pre, post;
     std::unique_ptr<SolverBase> coarse;
-    Hierarchy H;  // kept for export
+    std::shared_ptr<const Hierarchy> H;  // kept for export
+    // gpu_precond_f32 = 1 (preconditioner only): the finest level too is
+    // stored and smoothed in float; input and output are converted here
+    bool full32 = false;
+    DVec b32, x32;
     void build(const HCsr &A0, const DCsr *A0dev, const Params &P, const std::string &role,
-               int nv);
+               int nv, HierCache *cache);
     void solve(DVec &x, DVec &b, const std::vector<double> &conv) override;
 
   private:
@@ -88,7 +98,7 @@ struct SolverHierarchy {
     int NV = 1;
     std::unique_ptr<SolverBase> root;
     MultiGrid *mg = nullptr;  // the multigrid object, if any
-    void build(const Params &P, const HCsr &hA_, const DCsr *A_, int nv);
+    void build(const Params &P, const HCsr &hA_, const DCsr *A_, int nv, HierCache *cache);
     void solve(DVec &x, DVec &b);
 };
 

@@ -105,8 +105,11 @@ def test_krylov_variants(gpu, oracle, method, nv):
 
 
 @pytest.mark.parametrize("smoother,reduced", [("Jacobi", 0), ("Chebyshev", 0), ("HSGS", 0),
-                                              ("Chebyshev", 1), ("HSGS", 1), ("Jacobi", 1)])
+                                              ("Chebyshev", 1), ("HSGS", 1), ("Jacobi", 1),
+                                              ("Chebyshev", "full32"), ("HSGS", "full32")])
 def test_amg_preconditioner(gpu, oracle, smoother, reduced):
+    """reduced: 0 FP64 (XAMG), 1 XAMG's mg_reduced_precision (levels >= 1 in
+    float), "full32" every level in float with 2-byte relative columns."""
     row, col, val = gpu.generate_diffusion(7, 18, 17, 16, 1.0, 1.0, 0)
     nv = 4
     sm = {"method": smoother}
@@ -114,9 +117,13 @@ def test_amg_preconditioner(gpu, oracle, smoother, reduced):
         sm["polynomial_order"] = 2
     if smoother == "HSGS":
         sm["max_iters"] = 1
-    params = {"solver": {"method": "MergedPBiCGStab", "max_iters": 300, "rel_tolerance": 1e-8,
-                         "abs_tolerance": 0},
-              "preconditioner": dict(MG_BASE, method="MultiGrid", mg_reduced_precision=reduced),
+    prec = dict(MG_BASE, method="MultiGrid", mg_reduced_precision=int(reduced == 1))
+    solver = {"method": "MergedPBiCGStab", "max_iters": 300, "rel_tolerance": 1e-8,
+              "abs_tolerance": 0}
+    if reduced == "full32":
+        prec.update(gpu_precond_f32=1, gpu_index_compress=2)
+        solver["gpu_index_compress"] = 2
+    params = {"solver": solver, "preconditioner": prec,
               "pre_smoother": sm, "post_smoother": dict(sm), "coarse_grid_solver": {"method": "Direct"}}
     st, S = check(gpu, oracle, row, col, val, nv, params, seed=5)
     assert S.nlevels() >= 3
