@@ -1799,6 +1799,19 @@ static std::shared_ptr<Solver> make_basic(System &sys, const std::string &role, 
 
 static int setup(System &sys) {
     if (sys.A64.empty()) return -1;
+    // dictionary defaults (xamg_params_details.h:131-144): with a MultiGrid
+    // list present, missing smoother lists are Jacobi and the coarse grid
+    // solver is Direct
+    bool any_mg = false;
+    for (auto &l : sys.P.base) {
+        auto m = l.second.find("method");
+        if (m != l.second.end() && m->second == "MultiGrid") any_mg = true;
+    }
+    if (any_mg) {
+        if (!sys.P.has("pre_smoother")) sys.P.base["pre_smoother"]["method"] = "Jacobi";
+        if (!sys.P.has("post_smoother")) sys.P.base["post_smoother"]["method"] = "Jacobi";
+        if (!sys.P.has("coarse_grid_solver")) sys.P.base["coarse_grid_solver"]["method"] = "Direct";
+    }
     const std::string pre = sys.P.get("preconditioner", "method");
     const std::string sol = sys.P.get("solver", "method");
     const bool mg_solver = (sol == "MultiGrid");
@@ -1854,8 +1867,13 @@ static int setup(System &sys) {
         for (size_t nl = 0; nl < L; ++nl) {
             const uint64_t n = sys.levels[nl].A.nrows;
             if (nl == 0) {
-                M->mgbuf[0].push_back(make_vec<double>(n, sys.NV));
-                if (reduced) M->mgbuf[0].push_back(make_vec<float>(n, sys.NV));
+                if (sys.levels[0].reduced) {
+                    // every level in float: the level-0 residual is float too
+                    M->mgbuf[0].push_back(make_vec<float>(n, sys.NV));
+                } else {
+                    M->mgbuf[0].push_back(make_vec<double>(n, sys.NV));
+                    if (reduced) M->mgbuf[0].push_back(make_vec<float>(n, sys.NV));
+                }
             } else {
                 for (int i = 0; i < 3; ++i) {
                     Vec v;

@@ -113,6 +113,9 @@ struct DCsr {
     bool f32 = false;
     uint16_t hash = 0;
     DevBuf row, col, val;
+    // largest number of entries in one tile of 256/nv rows, per nv = 1..32
+    // (index log2 nv); 0 = not known yet
+    uint32_t tile_max[6] = {0, 0, 0, 0, 0, 0};
 
     template <typename F>
     k::CsrArgs<F> args() const {

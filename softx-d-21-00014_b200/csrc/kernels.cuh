@@ -180,13 +180,54 @@ __device__ __forceinline__ uint64_t col_of(const I *col, uint64_t j, uint64_t i)
         return (uint64_t)__ldg(&col[j]);
 }
 
+// Row accumulation in batches: the products x[c]*a of up to BATCH entries are
+// formed first (all gathers in flight at once), then added to y one by one in
+// entry order, so the rounding sequence is that of the plain loop.
+constexpr int BATCH = 8;
+constexpr int SPMV_MIN_BLOCKS = 3;  // occupancy floor: registers <= 85 per thread
+
+template <typename F, typename FX, typename I, int NV, bool STAGED>
+__device__ __forceinline__ F row_sum(F y, uint32_t a, uint32_t b, uint64_t i, int k,
+                                     const uint32_t *s_col, const F *s_val, const I *col,
+                                     const F *val, const FX *x) {
+    for (uint32_t j = a; j < b; j += BATCH) {
+        const uint32_t m = (b - j) < (uint32_t)BATCH ? (b - j) : (uint32_t)BATCH;
+        F pr[BATCH];
+#pragma unroll
+        for (int q = 0; q < BATCH; ++q) {
+            if ((uint32_t)q < m) {
+                uint64_t c;
+                F av;
+                if constexpr (STAGED) {
+                    if constexpr (std::is_same<I, int16_t>::value)
+                        c = (uint64_t)((int64_t)i + (int64_t)(int32_t)s_col[j + q]);
+                    else
+                        c = (uint64_t)s_col[j + q];
+                    av = s_val[j + q];
+                } else {
+                    c = col_of(col, j + q, i);
+                    av = __ldg(&val[j + q]);
+                }
+                pr[q] = mul((F)__ldg(&x[c * NV + k]), av);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < BATCH; ++q)
+            if ((uint32_t)q < m) y = add(y, pr[q]);
+    }
+    return y;
+}
+
+// Kernel with dynamic shared memory: cap entries of (value, u32 column)
+// staged per tile; tiles with more entries read global memory directly.
 template <typename F, typename FX, typename I, int NV, int NRED, class Epi>
-__global__ void __launch_bounds__(CT)
-    k_spmv(CsrArgs<F> A, const FX *__restrict__ x, Epi epi, RedArgs ra) {
+__global__ void __launch_bounds__(CT, SPMV_MIN_BLOCKS)
+    k_spmv(CsrArgs<F> A, const FX *__restrict__ x, Epi epi, RedArgs ra, uint32_t cap) {
     constexpr int R = CT / NV;
-    constexpr int CAP = StageCap<F>::value;
-    __shared__ F s_val[CAP];
-    __shared__ uint32_t s_col[CAP];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    F *s_val = (F *)smem_raw;
+    uint32_t *s_col = (uint32_t *)(smem_raw + (size_t)cap * sizeof(F));
+    const uint32_t CAP = cap;
     const int rt = threadIdx.x / NV, k = threadIdx.x % NV;
     const uint32_t *__restrict__ row = A.row;
     const I *__restrict__ col = (const I *)A.col;
@@ -201,12 +242,12 @@ __global__ void __launch_bounds__(CT)
         const uint64_t r1 = r0 + R < n ? r0 + R : n;
         const uint32_t tj0 = __ldg(&row[r0]), tj1 = __ldg(&row[r1]);
         const uint32_t cnt = tj1 - tj0;
-        const bool staged = cnt <= (uint32_t)CAP;
+        const bool staged = cnt <= CAP;
         __syncthreads();  // the previous tile's readers are done with the buffers
         if (staged) {
             // rows of this tile own [tj0, tj1); the row index of entry e is only
             // needed for the relative form, found by the owning thread below
-#pragma unroll 4
+#pragma unroll 8
             for (uint32_t e = threadIdx.x; e < cnt; e += CT) {
                 if constexpr (std::is_same<I, int16_t>::value)
                     s_col[e] = (uint32_t)(int32_t)__ldg(&col[tj0 + e]);
@@ -220,28 +261,27 @@ __global__ void __launch_bounds__(CT)
         if (i < n) {
             F y = epi.init(i, k);
             const uint32_t j0 = __ldg(&row[i]), j1 = __ldg(&row[i + 1]);
-            if (staged) {
-                const uint32_t a = j0 - tj0, b = j1 - tj0;
-#pragma unroll 4
-                for (uint32_t j = a; j < b; ++j) {
-                    uint64_t c;
-                    if constexpr (std::is_same<I, int16_t>::value)
-                        c = (uint64_t)((int64_t)i + (int64_t)(int32_t)s_col[j]);
-                    else
-                        c = (uint64_t)s_col[j];
-                    const F xv = (F)__ldg(&x[c * NV + k]);
-                    y = add(y, mul(xv, s_val[j]));
-                }
-            } else {
-                for (uint32_t j = j0; j < j1; ++j) {
-                    const F xv = (F)__ldg(&x[col_of(col, j, i) * NV + k]);
-                    y = add(y, mul(xv, __ldg(&val[j])));
-                }
-            }
+            if (staged)
+                y = row_sum<F, FX, I, NV, true>(y, j0 - tj0, j1 - tj0, i, k, s_col, s_val, col,
+                                                val, x);
+            else
+                y = row_sum<F, FX, I, NV, false>(y, j0, j1, i, k, s_col, s_val, col, val, x);
             epi.store(i, k, y, acc);
         }
     }
     if constexpr (NRED > 0) canon_finish<F, NV, NRED>(acc, ra, epi);
+}
+
+// Largest entry count of a tile of R rows (for matrices whose row pointers
+// live only on the device).
+static __global__ void k_tile_max(const uint32_t *__restrict__ row, uint64_t n, uint64_t R,
+                                  unsigned *out) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t r0 = t * R;
+    if (r0 < n) {
+        const uint64_t r1 = r0 + R < n ? r0 + R : n;
+        atomicMax(out, row[r1] - row[r0]);
+    }
 }
 
 // Element-wise canonical kernel (same schedule, no matrix).

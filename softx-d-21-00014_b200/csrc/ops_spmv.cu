@@ -1,5 +1,8 @@
 // Launchers of the CSR kernels: runtime (nv, column width) -> template
 // instantiation of k_spmv with the matching epilogue.
+#include <algorithm>
+#include <map>
+#include <tuple>
 #include <type_traits>
 
 #include "ops.h"
@@ -34,11 +37,49 @@ static void dispatch_col(int cb, Fn &&fn) {
     }
 }
 
+// Largest tile entry count for nv: known from the upload for library-owned
+// matrices; for caller-owned device descriptors computed once on the device
+// and remembered per (row pointer, rows). A stale value can only change which
+// tiles are staged, never a result.
+static uint32_t tile_max(const DCsr &A, int nv, cudaStream_t s) {
+    int l = 0;
+    while ((1 << l) < nv) ++l;
+    if (A.tile_max[l] || A.nnz == 0) return A.tile_max[l];
+    static std::map<std::tuple<const void *, uint64_t, int>, uint32_t> cache;
+    auto key = std::make_tuple((const void *)A.row.p, A.nrows, l);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    const uint64_t R = (uint64_t)k::CT >> l;
+    const uint64_t ntiles = (A.nrows + R - 1) / R;
+    unsigned *d = ctx().red_ticket.as<unsigned>() + 1;
+    XG_CUDA(cudaMemsetAsync(d, 0, sizeof(unsigned), s));
+    k::k_tile_max<<<(unsigned)((ntiles + 255) / 256), 256, 0, s>>>(A.row.as<uint32_t>(), A.nrows,
+                                                                     R, d);
+    XG_CUDA(cudaGetLastError());
+    unsigned h = 0;
+    XG_CUDA(cudaMemcpyAsync(&h, d, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    XG_CUDA(cudaStreamSynchronize(s));
+    cache[key] = h;
+    return h;
+}
+
 template <typename F, typename FX, typename I, int NV, int NRED, class Epi>
 static void launch(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s) {
     if (A.nrows == 0) return;
     const int B = k::canon_blocks(A.nrows, NV);
-    k::k_spmv<F, FX, I, NV, NRED, Epi><<<B, k::CT, 0, s>>>(A.args<F>(), x, epi, ctx().red());
+    // stage up to 96 KB of (value, column) pairs per tile: two blocks per SM
+    // even for the largest tiles
+    constexpr uint32_t LIMIT = (96u * 1024u) / (uint32_t)(sizeof(F) + 4);
+    const uint32_t cap = std::min(tile_max(A, NV, s), LIMIT);
+    const size_t smem = (size_t)cap * (sizeof(F) + 4);
+    auto kern = k::k_spmv<F, FX, I, NV, NRED, Epi>;
+    static bool big_smem = false;  // one flag per instantiation
+    if (smem > 48u * 1024u && !big_smem) {
+        XG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)((size_t)LIMIT * (sizeof(F) + 4))));
+        big_smem = true;
+    }
+    kern<<<B, k::CT, smem, s>>>(A.args<F>(), x, epi, ctx().red(), cap);
     XG_CUDA(cudaGetLastError());
     ++g_kernel_launches;
 }

@@ -1,5 +1,6 @@
 // Flat element-wise launchers, the process context, and CSR upload/download
 // with XAMG's index narrowing.
+#include <algorithm>
 #include <cstring>
 
 #include "ops.h"
@@ -153,6 +154,15 @@ void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s) {
                 }
             }
         if (fits) d.col_bytes = -2;
+    }
+    for (int l = 0; l < 6; ++l) {
+        const uint64_t R = (uint64_t)k::CT >> l;
+        uint32_t mx = 0;
+        for (uint64_t r0 = 0; r0 < h.nrows; r0 += R) {
+            const uint64_t r1 = std::min<uint64_t>(r0 + R, h.nrows);
+            mx = std::max<uint32_t>(mx, h.row[r1] - h.row[r0]);
+        }
+        d.tile_max[l] = mx;
     }
     upload(d.row, h.row, s);
     if (d.col_bytes == -2) {
