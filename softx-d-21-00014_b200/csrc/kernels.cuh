@@ -180,40 +180,30 @@ __device__ __forceinline__ uint64_t col_of(const I *col, uint64_t j, uint64_t i)
         return (uint64_t)__ldg(&col[j]);
 }
 
-// Row accumulation in batches: the products x[c]*a of up to BATCH entries are
-// formed first (all gathers in flight at once), then added to y one by one in
-// entry order, so the rounding sequence is that of the plain loop.
-constexpr int BATCH = 8;
-constexpr int SPMV_MIN_BLOCKS = 3;  // occupancy floor: registers <= 85 per thread
+// Row accumulation, entry by entry in row order (the loop is unrolled so that
+// gathers of later entries can issue before earlier sums complete; the
+// additions stay in order).
+constexpr int SPMV_MIN_BLOCKS = 1;
 
 template <typename F, typename FX, typename I, int NV, bool STAGED>
 __device__ __forceinline__ F row_sum(F y, uint32_t a, uint32_t b, uint64_t i, int k,
                                      const uint32_t *s_col, const F *s_val, const I *col,
                                      const F *val, const FX *x) {
-    for (uint32_t j = a; j < b; j += BATCH) {
-        const uint32_t m = (b - j) < (uint32_t)BATCH ? (b - j) : (uint32_t)BATCH;
-        F pr[BATCH];
-#pragma unroll
-        for (int q = 0; q < BATCH; ++q) {
-            if ((uint32_t)q < m) {
-                uint64_t c;
-                F av;
-                if constexpr (STAGED) {
-                    if constexpr (std::is_same<I, int16_t>::value)
-                        c = (uint64_t)((int64_t)i + (int64_t)(int32_t)s_col[j + q]);
-                    else
-                        c = (uint64_t)s_col[j + q];
-                    av = s_val[j + q];
-                } else {
-                    c = col_of(col, j + q, i);
-                    av = __ldg(&val[j + q]);
-                }
-                pr[q] = mul((F)__ldg(&x[c * NV + k]), av);
-            }
+#pragma unroll 4
+    for (uint32_t j = a; j < b; ++j) {
+        uint64_t c;
+        F av;
+        if constexpr (STAGED) {
+            if constexpr (std::is_same<I, int16_t>::value)
+                c = (uint64_t)((int64_t)i + (int64_t)(int32_t)s_col[j]);
+            else
+                c = (uint64_t)s_col[j];
+            av = s_val[j];
+        } else {
+            c = col_of(col, j, i);
+            av = __ldg(&val[j]);
         }
-#pragma unroll
-        for (int q = 0; q < BATCH; ++q)
-            if ((uint32_t)q < m) y = add(y, pr[q]);
+        y = add(y, mul((F)__ldg(&x[c * NV + k]), av));
     }
     return y;
 }
