@@ -183,7 +183,7 @@ __device__ __forceinline__ uint64_t col_of(const I *col, uint64_t j, uint64_t i)
 // Row accumulation, entry by entry in row order (the loop is unrolled so that
 // gathers of later entries can issue before earlier sums complete; the
 // additions stay in order).
-constexpr int SPMV_MIN_BLOCKS = 1;
+constexpr int SPMV_MIN_BLOCKS = 8;  // full occupancy: at most 32 registers per thread
 
 template <typename F, typename FX, typename I, int NV, bool STAGED>
 __device__ __forceinline__ F row_sum(F y, uint32_t a, uint32_t b, uint64_t i, int k,
@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(CT, SPMV_MIN_BLOCKS)
         if (staged) {
             // rows of this tile own [tj0, tj1); the row index of entry e is only
             // needed for the relative form, found by the owning thread below
-#pragma unroll 8
+#pragma unroll 4
             for (uint32_t e = threadIdx.x; e < cnt; e += CT) {
                 if constexpr (std::is_same<I, int16_t>::value)
                     s_col[e] = (uint32_t)(int32_t)__ldg(&col[tj0 + e]);
