@@ -73,6 +73,20 @@ int XAMG_b200_spmv_dot(const XAMG_b200_csr *A, const double *x, double *v, const
 int XAMG_b200_dot(uint64_t n, int nv, const double *x, const double *y, double *dot_out,
                   void *stream);
 
+/* The dot product of XAMG_b200_dot for callers that cannot allocate device
+ * memory (for example an application whose device memory is owned by its own
+ * pool allocator, or a latency-bound loop where a cudaMalloc, which may
+ * synchronise the device, is not allowed). No counterpart in the reference.
+ * It allocates nothing: its scratch is a fixed __device__ array of this
+ * library (1184 x 32 partial sums, 303,104 bytes, plus a counter) whose device
+ * address is looked up on the first call on each device, so that first call
+ * should precede any stream capture. x, y and dot_out (nv doubles) are device
+ * arrays; nv must be 1, 2, 4, 8, 16 or 32 (XAMG_ERR_INVALID_ARG otherwise).
+ * The result equals XAMG_b200_dot's bit for bit. All calls share the scratch:
+ * calls whose kernels overlap on the GPU race. */
+int XAMG_b200_dot_noalloc(uint64_t n, int nv, const double *x, const double *y, double *dot_out,
+                          void *stream);
+
 /* merged_bicgstab_group1/2/4 (blas_merged_bicgstab.inl:32-194) on device
  * arrays; the reductions come back in host arrays of nv values. */
 int XAMG_b200_group1(uint64_t n, int nv, double *r0, const double *b, double *p, double *r,

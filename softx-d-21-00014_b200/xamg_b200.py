@@ -54,7 +54,7 @@ EXT_SYMBOLS = [
     "XAMG_b200_solver_level_info", "XAMG_b200_solver_level_download",
     "XAMG_b200_solver_hierarchy_export", "XAMG_b200_vector_device_ptr",
     "XAMG_b200_solver_level_csr", "XAMG_b200_kernel_launches", "XAMG_b200_stream",
-    "XAMG_b200_set_device",
+    "XAMG_b200_set_device", "XAMG_b200_dot_noalloc",
 ]
 
 
@@ -148,6 +148,7 @@ def lib():
         "XAMG_b200_spmv": (C.c_int, [C.POINTER(Csr), vp, vp, C.c_int, C.c_int, vp]),
         "XAMG_b200_spmv_dot": (C.c_int, [C.POINTER(Csr), vp, vp, vp, vp, C.c_int, vp]),
         "XAMG_b200_dot": (C.c_int, [u64, C.c_int, vp, vp, vp, vp]),
+        "XAMG_b200_dot_noalloc": (C.c_int, [u64, C.c_int, vp, vp, vp, vp]),
         "XAMG_b200_group1": (C.c_int, [u64, C.c_int, vp, vp, vp, vp, vp, vp]),
         "XAMG_b200_group2": (C.c_int, [u64, C.c_int, vp, vp, vp, vp, vp, vp]),
         "XAMG_b200_group4": (C.c_int, [u64, C.c_int, vp, vp, vp, vp, vp, vp, vp]),
