@@ -162,6 +162,14 @@ int XAMG_b200_set_device(int device);
 /* Device address of a vector's [size][nv] storage (no counterpart). */
 int XAMG_b200_vector_device_ptr(size_t vid, void **ptr);
 
+/* Exercises the bounded waits of the library's kernels (no counterpart): a
+ * kernel waits on a barrier that nothing completes, gives up after `seconds`
+ * (at most 1) and raises the timeout flag that every solve checks; on return
+ * *timed_out is 1 and the GPU context is still usable. Kernels that stage
+ * matrix entries wait at most 2 s per copy and report XAMG_ERR_TIMEOUT from
+ * the solve call. */
+int XAMG_b200_wait_selftest(double seconds, int *timed_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -594,6 +594,7 @@ static void do_solve(SolverObj &so, VecObj &x, VecObj &b, int nv) {
                "vector size differs from the matrix size");
     if (nv != so.nv) build_solver(so, so.sh->params, nv);
     so.sh->solve(x.v, b.v);
+    ctx().check_flags();
 }
 
 int XAMG_solver_solve1(uint16_t nv, XAMG_solver_id sid) {
@@ -883,6 +884,22 @@ int XAMG_b200_vector_device_ptr(size_t vid, void **ptr) {
         VecObj &v = get(g_vecs, vid, "vector");
         XG_REQUIRE(ptr, XAMG_ERR_INVALID_ARG, "null pointer");
         *ptr = v.v.p<double>();
+    });
+}
+
+int XAMG_b200_wait_selftest(double seconds, int *timed_out) {
+    return guarded([&] {
+        XG_REQUIRE(timed_out && seconds > 0 && seconds <= 1.0, XAMG_ERR_INVALID_ARG,
+                   "seconds must be in (0, 1]");
+        Ctx &c = ctx();
+        *timed_out = 0;
+        ops::wait_selftest((uint64_t)(seconds * 1e9), c.stream);
+        try {
+            c.check_flags();
+        } catch (const Error &e) {
+            if (e.code != XAMG_ERR_TIMEOUT) throw;
+            *timed_out = 1;
+        }
     });
 }
 

@@ -62,7 +62,8 @@ struct DevBuf {
 struct Ctx {
     cudaStream_t stream = nullptr;
     DevBuf red_part;    // canonical-reduction partials: BMAX x 32 x 3 doubles
-    DevBuf red_ticket;  // one counter, zero between launches
+    DevBuf red_ticket;  // [0] reduction counter (zero between launches),
+                        // [1] tile-size scratch, [2] wait-timeout flag
     DevBuf red_out;     // 96 doubles for reductions returned to the host
     double *pinned = nullptr;  // 256 doubles of pinned host memory
     int device = 0;
@@ -71,7 +72,12 @@ struct Ctx {
 
     void init();
     void shutdown();
-    k::RedArgs red() const { return k::RedArgs{red_part.p, red_ticket.as<unsigned>()}; }
+    k::RedArgs red() const {
+        return k::RedArgs{red_part.p, red_ticket.as<unsigned>(), red_ticket.as<unsigned>() + 2};
+    }
+    // Throws XAMG_ERR_TIMEOUT (and clears the flag) if a kernel's bounded wait
+    // ran out since the last check; synchronises the stream.
+    void check_flags();
 };
 
 Ctx &ctx();

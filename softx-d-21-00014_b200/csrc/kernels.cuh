@@ -15,7 +15,9 @@
 //
 // Row schedule ("canonical order"): a block has 256 threads; thread t works on
 // row slot t/NV and right-hand side t%NV, so a tile covers 256/NV consecutive
-// rows and consecutive threads read consecutive x entries of a row. Tiles are
+// rows and consecutive threads read consecutive x entries of a row. (The SpMV
+// runs these 256 canonical threads on 256/VK physical ones, each carrying VK
+// consecutive right-hand sides; see canon_finish.) Tiles are
 // dealt round-robin to B = min(ntiles, 1184) blocks (8 per SM on 148 SMs).
 // Dot products are accumulated per thread in tile order, combined within a
 // warp by an xor butterfly (offsets 16..NV), across the 8 warps in warp
@@ -97,27 +99,43 @@ inline int canon_blocks(uint64_t n, int nv) {
 // Canonical reduction: block partials, then the last block finishes.
 // ---------------------------------------------------------------------------
 struct RedArgs {
-    void *part;        // [BMAX][32][3] partial sums (element type of the kernel)
-    unsigned *ticket;  // zero between launches
+    void *part;              // [BMAX][32][3] partial sums (element type of the kernel)
+    unsigned *ticket;        // zero between launches
+    unsigned *flag = nullptr;  // bit 0: a bounded wait ran out (read by the host)
 };
 
-template <typename T, int NV, int NRED, class Fin>
-__device__ __forceinline__ void canon_finish(T (&acc)[NRED], const RedArgs &ra, const Fin &fin) {
+// A block may run the 256 canonical threads with CT/VK physical threads:
+// physical thread p plays canonical threads p*VK .. p*VK+VK-1 (right-hand
+// sides k0 .. k0+VK-1 of one row slot) and keeps one accumulator per
+// canonical thread. Canonical warp w is then physical threads
+// [w*32/VK, (w+1)*32/VK), and a canonical butterfly offset `off` (a multiple
+// of VK, since off >= NV >= VK) is the physical offset off/VK, so every sum is
+// formed from the same operands in the same order as with VK = 1.
+template <typename T, int NV, int NRED, int VK, class Fin>
+__device__ __forceinline__ void canon_finish(T (&acc)[VK][NRED], const RedArgs &ra,
+                                             const Fin &fin) {
+    constexpr int NT = CT / VK;   // physical threads of the block
+    constexpr int NW = NT / 32;   // physical warps
+    constexpr int SUB = 32 / VK;  // physical threads of one canonical warp
+    constexpr int G = NV / VK;    // physical threads of one row slot
     __shared__ T wsum[8 * NV * NRED];
     __shared__ T sums[NV * NRED];
     __shared__ int is_last;
     T *part = (T *)ra.part;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int cw = threadIdx.x / SUB, cl = threadIdx.x % SUB;  // canonical lane = cl*VK + v
 #pragma unroll
-    for (int r = 0; r < NRED; ++r) {
-        T v = acc[r];
+    for (int v = 0; v < VK; ++v) {
 #pragma unroll
-        for (int off = 16; off >= NV; off >>= 1) v = add(v, shfl_xor(v, off));
-        if (lane < NV) wsum[(warp * NV + lane) * NRED + r] = v;
+        for (int r = 0; r < NRED; ++r) {
+            T s = acc[v][r];
+#pragma unroll
+            for (int off = 16; off >= NV; off >>= 1) s = add(s, shfl_xor(s, off / VK));
+            if (cl < G) wsum[(cw * NV + cl * VK + v) * NRED + r] = s;
+        }
     }
     __syncthreads();
-    if (threadIdx.x < NV * NRED) {
-        const int o = threadIdx.x;  // o = k*NRED + r
+    for (int o = threadIdx.x; o < NV * NRED; o += NT) {  // o = k*NRED + r
         T s = wsum[o];
 #pragma unroll
         for (int w = 1; w < 8; ++w) s = add(s, wsum[w * NV * NRED + o]);
@@ -132,7 +150,7 @@ __device__ __forceinline__ void canon_finish(T (&acc)[NRED], const RedArgs &ra, 
     __syncthreads();
     if (!is_last) return;
     __threadfence();
-    for (int o = warp; o < NV * NRED; o += 8) {
+    for (int o = warp; o < NV * NRED; o += NW) {
         T a = T(0);
         for (unsigned bb = lane; bb < gridDim.x; bb += 32)
             a = add(a, ld_cg(&part[(size_t)bb * NV * NRED + o]));
@@ -142,7 +160,12 @@ __device__ __forceinline__ void canon_finish(T (&acc)[NRED], const RedArgs &ra, 
     }
     __syncthreads();
     if (threadIdx.x == 0) *ra.ticket = 0u;
-    if (threadIdx.x < NV) fin(threadIdx.x, &sums[threadIdx.x * NRED]);
+    for (int kk = threadIdx.x; kk < NV; kk += NT) fin(kk, &sums[kk * NRED]);
+}
+
+template <typename T, int NV, int NRED, class Fin>
+__device__ __forceinline__ void canon_finish(T (&acc)[NRED], const RedArgs &ra, const Fin &fin) {
+    canon_finish<T, NV, NRED, 1>(reinterpret_cast<T(&)[1][NRED]>(acc), ra, fin);
 }
 
 // ---------------------------------------------------------------------------
@@ -160,106 +183,296 @@ struct CsrArgs {
     uint64_t n;
 };
 
-// Shared-memory staging: a tile's entries [row[r0], row[r0+R]) are copied into
-// shared memory by all 256 threads with coalesced loads (many loads in flight
-// per thread), then every thread walks its own row from shared memory. Tiles
-// with more entries than the staging capacity read global memory directly.
-template <typename F>
-struct StageCap {
-    static constexpr int value = sizeof(F) == 8 ? 2048 : 3072;  // 24 KB per block
-};
+// Shared-memory staging: a tile's entries [row[r0], row[r0+R]) (values and
+// columns in their stored types) are copied into shared memory by the bulk
+// copy engine (cp.async.bulk, completion on an mbarrier), double-buffered so
+// that the copy of a block's next tile overlaps the work on the current one;
+// every thread then walks its own row from shared memory. The copy takes the
+// 16-byte-aligned part of each array range; the few entries outside it (at an
+// array's unaligned start or end) are copied with plain loads by the issuing
+// thread before it arrives on the barrier. Tiles with more entries than the
+// staging capacity read global memory directly.
 
 // Column index of entry j: narrowed absolute index (I unsigned) or, for
 // I = int16_t, a signed offset from the row index (the 2-byte relative form
 // used where every |col - row| < 32768).
 template <typename I>
-__device__ __forceinline__ uint64_t col_of(const I *col, uint64_t j, uint64_t i) {
+__device__ __forceinline__ uint64_t col_at(I c, uint64_t i) {
     if constexpr (std::is_same<I, int16_t>::value)
-        return (uint64_t)((int64_t)i + (int64_t)__ldg(&col[j]));
+        return (uint64_t)((int64_t)i + (int64_t)c);
     else
-        return (uint64_t)__ldg(&col[j]);
+        return (uint64_t)c;
+}
+
+// Right-hand sides one SpMV thread carries: x[c*NV + k0 .. k0+VK-1] is one
+// aligned load of at most 16 bytes, so a warp issues 1/VK of the
+// shared-memory reads of (column, value) and of the gather instructions that
+// a thread per right-hand side would. The canonical order does not change
+// (canon_finish).
+#ifndef XG_SPMV_VK
+#define XG_SPMV_VK 2
+#endif
+template <typename FX, int NV>
+__host__ __device__ constexpr int spmv_vk() {
+    constexpr int w = 16 / (int)sizeof(FX) < XG_SPMV_VK ? 16 / (int)sizeof(FX) : XG_SPMV_VK;
+    return NV < w ? NV : w;
+}
+
+template <typename FX, int VK>
+__device__ __forceinline__ void ld_x(const FX *p, FX (&o)[VK]) {
+    if constexpr (VK == 1) {
+        o[0] = __ldg(p);
+    } else if constexpr (std::is_same<FX, double>::value) {
+#pragma unroll
+        for (int h = 0; h < VK; h += 2) {
+            const double2 t = __ldg(reinterpret_cast<const double2 *>(p + h));
+            o[h] = t.x;
+            o[h + 1] = t.y;
+        }
+    } else if constexpr (VK == 2) {
+        const float2 t = __ldg(reinterpret_cast<const float2 *>(p));
+        o[0] = t.x;
+        o[1] = t.y;
+    } else {
+#pragma unroll
+        for (int h = 0; h < VK; h += 4) {
+            const float4 t = __ldg(reinterpret_cast<const float4 *>(p + h));
+            o[h] = t.x;
+            o[h + 1] = t.y;
+            o[h + 2] = t.z;
+            o[h + 3] = t.w;
+        }
+    }
 }
 
 // Row accumulation, entry by entry in row order (the loop is unrolled so that
 // gathers of later entries can issue before earlier sums complete; the
-// additions stay in order).
-constexpr int SPMV_MIN_BLOCKS = 8;  // full occupancy: at most 32 registers per thread
+// additions stay in order). cl/vl point at the row's first entry.
+// Resident blocks the register budget allows: at most 64 registers a thread
+// (a block of 256 threads also needs a 40 KB staging pair, so no more than
+// five fit an SM anyway).
+template <int VK>
+constexpr int spmv_min_blocks() { return VK == 1 ? 4 : 8; }
 
-template <typename F, typename FX, typename I, int NV, bool STAGED>
-__device__ __forceinline__ F row_sum(F y, uint32_t a, uint32_t b, uint64_t i, int k,
-                                     const uint32_t *s_col, const F *s_val, const I *col,
-                                     const F *val, const FX *x) {
+template <typename F, typename FX, typename I, int NV, int VK>
+__device__ __forceinline__ void row_sum(F (&y)[VK], uint32_t len, uint64_t i, int k0, const I *cl,
+                                        const F *vl, const FX *x) {
 #pragma unroll 4
-    for (uint32_t j = a; j < b; ++j) {
-        uint64_t c;
-        F av;
-        if constexpr (STAGED) {
-            if constexpr (std::is_same<I, int16_t>::value)
-                c = (uint64_t)((int64_t)i + (int64_t)(int32_t)s_col[j]);
-            else
-                c = (uint64_t)s_col[j];
-            av = s_val[j];
-        } else {
-            c = col_of(col, j, i);
-            av = __ldg(&val[j]);
-        }
-        y = add(y, mul((F)__ldg(&x[c * NV + k]), av));
+    for (uint32_t j = 0; j < len; ++j) {
+        const uint64_t c = col_at<I>(cl[j], i);
+        const F av = vl[j];
+        FX xv[VK];
+        ld_x<FX, VK>(x + c * NV + k0, xv);
+#pragma unroll
+        for (int v = 0; v < VK; ++v) y[v] = add(y[v], mul((F)xv[v], av));
     }
-    return y;
 }
 
-// Kernel with dynamic shared memory: cap entries of (value, u32 column)
-// staged per tile; tiles with more entries read global memory directly.
-template <typename F, typename FX, typename I, int NV, int NRED, class Epi>
-__global__ void __launch_bounds__(CT, SPMV_MIN_BLOCKS)
-    k_spmv(CsrArgs<F> A, const FX *__restrict__ x, Epi epi, RedArgs ra, uint32_t cap) {
+// --- mbarrier and bulk-copy primitives (PTX) -------------------------------
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *m, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(m)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect(uint64_t *m, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(m)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *m, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(m)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Waits for phase `parity` of the barrier for at most limit_ns nanoseconds
+// of the global timer (and a bounded number of polls); false if the limit ran
+// out.
+constexpr uint64_t WAIT_LIMIT_NS = 2000000000ull;
+__device__ __forceinline__ bool mbar_wait(uint64_t *m, uint32_t parity,
+                                          uint64_t limit_ns = WAIT_LIMIT_NS) {
+    if (mbar_try_wait(m, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (uint32_t it = 0; it < (1u << 30); ++it) {
+        if (mbar_try_wait(m, parity)) return true;
+        if (global_ns() - t0 > limit_ns) return false;
+    }
+    return false;
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes,
+                                         uint64_t *m) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+        "[%3];" ::"r"(smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(m))
+        : "memory");
+}
+
+// Staging plan of entries [j0, j1) of an array of n elements of T: the
+// 16-byte-aligned global range [c0, c1) goes by bulk copy (src/dst/return
+// value: its source, destination and byte count) and entry j lands at
+// sbuf[j - j0 + stage_shift(arr, j0)]; entries outside [c0, c1) are copied
+// here with plain loads.
+template <typename T>
+__device__ __forceinline__ uint32_t stage_range(T *sbuf, const T *arr, uint64_t n, uint32_t j0,
+                                                uint32_t j1, const T *&src, T *&dst) {
+    constexpr uintptr_t A16 = 15;
+    const uintptr_t base = (uintptr_t)arr, end = (uintptr_t)(arr + n);
+    const uintptr_t lo = (uintptr_t)(arr + j0), hi = (uintptr_t)(arr + j1);
+    const uintptr_t g0 = lo & ~A16;
+    const uintptr_t b16 = (base + A16) & ~A16, e16 = end & ~A16, h16 = (hi + A16) & ~A16;
+    uintptr_t c0 = g0 > b16 ? g0 : b16;
+    uintptr_t c1 = h16 < e16 ? h16 : e16;
+    if (c1 <= c0) c0 = c1 = lo;  // nothing aligned to copy in bulk
+    T *s0 = sbuf + (lo - g0) / sizeof(T);  // s0[j - j0] is entry j's slot
+    const uint32_t cnt = j1 - j0;
+    uint32_t head = c0 > lo ? (uint32_t)((c0 - lo) / sizeof(T)) : 0u;  // entries before c0
+    if (head > cnt) head = cnt;
+    for (uint32_t e = 0; e < head; ++e) s0[e] = arr[j0 + e];
+    uint32_t tail = c1 > lo ? (uint32_t)((c1 - lo) / sizeof(T)) : 0u;  // first entry at/after c1
+    if (tail < head) tail = head;
+    for (uint32_t e = tail; e < cnt; ++e) s0[e] = arr[j0 + e];
+    src = (const T *)c0;
+    dst = sbuf + (c0 - g0) / sizeof(T);
+    return (uint32_t)(c1 - c0);
+}
+
+template <typename T>
+__device__ __forceinline__ uint32_t stage_shift(const T *arr, uint32_t j0) {
+    return (uint32_t)(((uintptr_t)(arr + j0) & 15) / sizeof(T));
+}
+
+// Kernel with dynamic shared memory: nbuf (1 or 2) buffers, each of cap
+// entries of values and columns plus 32 bytes of alignment slack per array;
+// tiles with more entries read global memory directly.
+// CT/VK threads; thread p carries row slot p/(NV/VK) and right-hand sides
+// k0 = (p % (NV/VK))*VK .. k0+VK-1 (x aligned to VK elements).
+template <typename F, typename FX, typename I, int NV, int VK, int NRED, class Epi>
+__global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
+    k_spmv(CsrArgs<F> A, const FX *__restrict__ x, Epi epi, RedArgs ra, uint32_t cap,
+           uint32_t nbuf) {
+    constexpr int G = NV / VK;
     constexpr int R = CT / NV;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    F *s_val = (F *)smem_raw;
-    uint32_t *s_col = (uint32_t *)(smem_raw + (size_t)cap * sizeof(F));
+    constexpr int NR = NRED > 0 ? NRED : 1;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t mbar[2];
+    const uint32_t VB = ((cap * (uint32_t)sizeof(F) + 32u) + 15u) & ~15u;
+    const uint32_t BB = VB + (((cap * (uint32_t)sizeof(I) + 32u) + 15u) & ~15u);
     const uint32_t CAP = cap;
-    const int rt = threadIdx.x / NV, k = threadIdx.x % NV;
+    const int rt = threadIdx.x / G, k0 = (threadIdx.x % G) * VK;
     const uint32_t *__restrict__ row = A.row;
     const I *__restrict__ col = (const I *)A.col;
     const F *__restrict__ val = A.val;
     const uint64_t n = A.n;
+    const uint64_t nnz = n ? row[n] : 0;
     const uint64_t ntiles = (n + R - 1) / R;
-    F acc[NRED > 0 ? NRED : 1];
+    F acc[VK][NR];
 #pragma unroll
-    for (int r = 0; r < (NRED > 0 ? NRED : 1); ++r) acc[r] = F(0);
+    for (int v = 0; v < VK; ++v)
+#pragma unroll
+        for (int r = 0; r < NR; ++r) acc[v][r] = F(0);
+
+    if (threadIdx.x == 0) {
+        mbar_init(&mbar[0], 1);
+        mbar_init(&mbar[1], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    uint32_t n_issued = 0, n_used = 0;  // staged tiles issued (thread 0) / consumed
+    bool timed_out = false;
+    // thread 0: copy tile t into the next buffer if it fits
+    auto issue = [&](uint64_t t) {
+        if (t >= ntiles) return;
+        const uint64_t a0 = t * R, a1 = a0 + R < n ? a0 + R : n;
+        const uint32_t j0 = row[a0], j1 = row[a1];
+        if (j1 - j0 > CAP) return;
+        unsigned char *buf = smem_raw + (size_t)(n_issued % nbuf) * BB;
+        uint64_t *m = &mbar[n_issued % nbuf];
+        ++n_issued;
+        const F *vsrc;
+        F *vdst;
+        const I *csrc;
+        I *cdst;
+        const uint32_t vb = stage_range<F>((F *)buf, val, nnz, j0, j1, vsrc, vdst);
+        const uint32_t cb = stage_range<I>((I *)(buf + VB), col, nnz, j0, j1, csrc, cdst);
+        mbar_arrive_expect(m, vb + cb);  // releases the plain-load writes above
+        fence_proxy_async_smem();
+        if (vb) bulk_g2s(vdst, vsrc, vb, m);
+        if (cb) bulk_g2s(cdst, csrc, cb, m);
+    };
+    if (threadIdx.x == 0) issue(blockIdx.x);
+
     for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const uint64_t r0 = tile * R;
         const uint64_t r1 = r0 + R < n ? r0 + R : n;
         const uint32_t tj0 = __ldg(&row[r0]), tj1 = __ldg(&row[r1]);
-        const uint32_t cnt = tj1 - tj0;
-        const bool staged = cnt <= CAP;
-        __syncthreads();  // the previous tile's readers are done with the buffers
+        const bool staged = tj1 - tj0 <= CAP;
+        if (nbuf == 2 && threadIdx.x == 0) issue(tile + gridDim.x);
+        const F *sv = nullptr;
+        const I *sc = nullptr;
         if (staged) {
-            // rows of this tile own [tj0, tj1); the row index of entry e is only
-            // needed for the relative form, found by the owning thread below
-#pragma unroll 4
-            for (uint32_t e = threadIdx.x; e < cnt; e += CT) {
-                if constexpr (std::is_same<I, int16_t>::value)
-                    s_col[e] = (uint32_t)(int32_t)__ldg(&col[tj0 + e]);
-                else
-                    s_col[e] = (uint32_t)__ldg(&col[tj0 + e]);
-                s_val[e] = __ldg(&val[tj0 + e]);
-            }
-            __syncthreads();
+            const uint32_t b = n_used % nbuf;
+            if (!mbar_wait(&mbar[b], (n_used / nbuf) & 1u)) timed_out = true;
+            ++n_used;
+            const unsigned char *buf = smem_raw + (size_t)b * BB;
+            sv = (const F *)buf + stage_shift<F>(val, tj0);
+            sc = (const I *)(buf + VB) + stage_shift<I>(col, tj0);
         }
         const uint64_t i = r0 + rt;
         if (i < n) {
-            F y = epi.init(i, k);
+            F y[VK];
+#pragma unroll
+            for (int v = 0; v < VK; ++v) y[v] = epi.init(i, k0 + v);
             const uint32_t j0 = __ldg(&row[i]), j1 = __ldg(&row[i + 1]);
             if (staged)
-                y = row_sum<F, FX, I, NV, true>(y, j0 - tj0, j1 - tj0, i, k, s_col, s_val, col,
-                                                val, x);
+                row_sum<F, FX, I, NV, VK>(y, j1 - j0, i, k0, sc + (j0 - tj0), sv + (j0 - tj0), x);
             else
-                y = row_sum<F, FX, I, NV, false>(y, j0, j1, i, k, s_col, s_val, col, val, x);
-            epi.store(i, k, y, acc);
+                row_sum<F, FX, I, NV, VK>(y, j1 - j0, i, k0, col + j0, val + j0, x);
+#pragma unroll
+            for (int v = 0; v < VK; ++v) epi.store(i, k0 + v, y[v], acc[v]);
         }
+        __syncthreads();  // every reader is done with this tile's buffer
+        if (nbuf == 1 && threadIdx.x == 0) issue(tile + gridDim.x);
     }
-    if constexpr (NRED > 0) canon_finish<F, NV, NRED>(acc, ra, epi);
+    if (timed_out) {
+        atomicOr(ra.flag, 1u);
+        // no block exits with a copy into its shared memory still in flight
+        if (threadIdx.x == 0)
+            for (uint32_t u = n_used; u < n_issued; ++u) mbar_wait(&mbar[u % nbuf], (u / nbuf) & 1u);
+    }
+    if constexpr (NRED > 0) canon_finish<F, NV, NRED, VK>(acc, ra, epi);
+}
+
+// Bounded-wait check: one block waits on an mbarrier that nothing arrives
+// at, gives up after limit_ns and raises the timeout flag, as a staging wait
+// of k_spmv does when its copy never lands. Nothing is in flight when it
+// returns.
+static __global__ void k_wait_selftest(uint64_t limit_ns, unsigned *flag) {
+    __shared__ __align__(8) uint64_t m;
+    if (threadIdx.x == 0) {
+        mbar_init(&m, 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    if (!mbar_wait(&m, 0, limit_ns) && threadIdx.x == 0) atomicOr(flag, 1u);
 }
 
 // Largest entry count of a tile of R rows (for matrices whose row pointers

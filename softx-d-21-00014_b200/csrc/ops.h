@@ -11,6 +11,9 @@ namespace ops {
 
 // --- SpMV family (blas2) ----------------------------------------------------
 // y = A x  /  y += A x   (csr_matvec.inl:148-260 / 32-144)
+// Launches a wait that must run out after limit_ns (raises the timeout flag).
+void wait_selftest(uint64_t limit_ns, cudaStream_t s);
+
 template <typename F>
 void spmv(const DCsr &A, const F *x, F *y, int nv, bool axpy, cudaStream_t s);
 

@@ -63,25 +63,56 @@ static uint32_t tile_max(const DCsr &A, int nv, cudaStream_t s) {
     return h;
 }
 
-template <typename F, typename FX, typename I, int NV, int NRED, class Epi>
-static void launch(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s) {
-    if (A.nrows == 0) return;
+// Staging buffers: one buffer holds cap entries of values and columns (plus
+// alignment slack); two buffers (the copy of the next tile overlapping the
+// current one) while they fit in 48 KB, at least four blocks per SM; else one
+// buffer of up to 96 KB.
+template <typename F, typename I>
+static uint32_t stage_buffer_bytes(uint32_t cap) {
+    auto r16 = [](uint64_t b) { return (uint32_t)((b + 15) & ~(uint64_t)15); };
+    return r16((uint64_t)cap * sizeof(F) + 32) + r16((uint64_t)cap * sizeof(I) + 32);
+}
+
+template <typename F, typename FX, typename I, int NV, int VK, int NRED, class Epi>
+static void launch_vk(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s) {
     const int B = k::canon_blocks(A.nrows, NV);
-    // stage up to 96 KB of (value, column) pairs per tile: two blocks per SM
-    // even for the largest tiles
-    constexpr uint32_t LIMIT = (96u * 1024u) / (uint32_t)(sizeof(F) + 4);
-    const uint32_t cap = std::min(tile_max(A, NV, s), LIMIT);
-    const size_t smem = (size_t)cap * (sizeof(F) + 4);
-    auto kern = k::k_spmv<F, FX, I, NV, NRED, Epi>;
+    constexpr uint32_t LIMIT1 = (96u * 1024u - 64u) / (uint32_t)(sizeof(F) + sizeof(I));
+    const uint32_t tm = tile_max(A, NV, s);
+    uint32_t cap = tm, nbuf = 2;
+    if (2 * stage_buffer_bytes<F, I>(tm) > 48u * 1024u) {
+        nbuf = 1;
+        cap = std::min(tm, LIMIT1);
+    }
+    const size_t smem = (size_t)nbuf * stage_buffer_bytes<F, I>(cap);
+    auto kern = k::k_spmv<F, FX, I, NV, VK, NRED, Epi>;
     static bool big_smem = false;  // one flag per instantiation
     if (smem > 48u * 1024u && !big_smem) {
         XG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)((size_t)LIMIT * (sizeof(F) + 4))));
+                                     (int)stage_buffer_bytes<F, I>(LIMIT1)));
         big_smem = true;
     }
-    kern<<<B, k::CT, smem, s>>>(A.args<F>(), x, epi, ctx().red(), cap);
+    kern<<<B, k::CT / VK, smem, s>>>(A.args<F>(), x, epi, ctx().red(), cap, nbuf);
     XG_CUDA(cudaGetLastError());
     ++g_kernel_launches;
+}
+
+// Vector loads of x need x aligned to VK elements; library vectors always are
+// (cudaMalloc). The entry points that take a caller's x (CALLER_X) fall back
+// to one right-hand side per thread for an x that is not (same results, same
+// reduction order).
+template <typename F, typename FX, typename I, int NV, int NRED, bool CALLER_X = false,
+          class Epi>
+static void launch(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s) {
+    if (A.nrows == 0) return;
+    constexpr int VK = k::spmv_vk<FX, NV>();
+    constexpr uintptr_t ALIGN = VK * sizeof(FX);
+    if (VK == 1 || (uintptr_t)x % ALIGN == 0) {
+        launch_vk<F, FX, I, NV, VK, NRED>(A, x, epi, s);
+    } else if constexpr (CALLER_X) {
+        launch_vk<F, FX, I, NV, 1, NRED>(A, x, epi, s);
+    } else {
+        throw Error(XAMG_ERR_INTERNAL, "library vector not aligned for the SpMV gather");
+    }
 }
 
 template <typename F, int NV, int NRED, class Epi>
@@ -102,13 +133,19 @@ static void launch_rows(uint64_t n, const Epi &epi, cudaStream_t s) {
         });                                                                 \
     })
 
+void wait_selftest(uint64_t limit_ns, cudaStream_t s) {
+    k::k_wait_selftest<<<1, 32, 0, s>>>(limit_ns, ctx().red().flag);
+    XG_CUDA(cudaGetLastError());
+    ++g_kernel_launches;
+}
+
 template <typename F>
 void spmv(const DCsr &A, const F *x, F *y, int nv, bool axpy, cudaStream_t s) {
     XG_DISPATCH(A, nv, {
         if (axpy)
-            launch<F, F, I, NV, 0>(A, x, k::EAxpy<F, NV>{{}, y}, s);
+            launch<F, F, I, NV, 0, true>(A, x, k::EAxpy<F, NV>{{}, y}, s);
         else
-            launch<F, F, I, NV, 0>(A, x, k::EStore<F, NV>{{}, y}, s);
+            launch<F, F, I, NV, 0, true>(A, x, k::EStore<F, NV>{{}, y}, s);
     });
 }
 template void spmv<double>(const DCsr &, const double *, double *, int, bool, cudaStream_t);
@@ -173,7 +210,7 @@ void group1_zero(uint64_t n, const double *b, double *r0, double *p, double *r, 
 void spmv_dot_alpha(const DCsr &A, const double *pa, double *v, const double *r0, double *sc,
                     int nv, cudaStream_t s) {
     XG_DISPATCH(A, nv, {
-        launch<double, double, I, NV, 1>(A, pa, k::EDotAlpha<NV>{v, r0, sc}, s);
+        launch<double, double, I, NV, 1, true>(A, pa, k::EDotAlpha<NV>{v, r0, sc}, s);
     });
 }
 

@@ -36,6 +36,18 @@ void Ctx::init() {
     ready = true;
 }
 
+void Ctx::check_flags() {
+    unsigned *pf = (unsigned *)(pinned + 255);
+    XG_CUDA(cudaMemcpyAsync(pf, red_ticket.as<unsigned>() + 2, sizeof(unsigned),
+                            cudaMemcpyDeviceToHost, stream));
+    XG_CUDA(cudaStreamSynchronize(stream));
+    if (*pf) {
+        XG_CUDA(cudaMemsetAsync(red_ticket.as<unsigned>() + 2, 0, sizeof(unsigned), stream));
+        XG_CUDA(cudaStreamSynchronize(stream));
+        throw Error(XAMG_ERR_TIMEOUT, "a kernel gave up waiting for its staged matrix entries");
+    }
+}
+
 void Ctx::shutdown() {
     if (!ready) return;
     cudaStreamSynchronize(stream);

@@ -54,7 +54,7 @@ EXT_SYMBOLS = [
     "XAMG_b200_solver_level_info", "XAMG_b200_solver_level_download",
     "XAMG_b200_solver_hierarchy_export", "XAMG_b200_vector_device_ptr",
     "XAMG_b200_solver_level_csr", "XAMG_b200_kernel_launches", "XAMG_b200_stream",
-    "XAMG_b200_set_device", "XAMG_b200_dot_noalloc",
+    "XAMG_b200_set_device", "XAMG_b200_dot_noalloc", "XAMG_b200_wait_selftest",
 ]
 
 
@@ -168,6 +168,7 @@ def lib():
         "XAMG_b200_kernel_launches": (C.c_uint64, []),
         "XAMG_b200_stream": (vp, []),
         "XAMG_b200_set_device": (C.c_int, [C.c_int]),
+        "XAMG_b200_wait_selftest": (C.c_int, [C.c_double, C.POINTER(C.c_int)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
