@@ -67,6 +67,7 @@ struct Ctx {
     DevBuf red_out;     // 96 doubles for reductions returned to the host
     double *pinned = nullptr;  // 256 doubles of pinned host memory
     int device = 0;
+    int sms = 148;            // streaming multiprocessors of the device
     int device_request = -1;  // set by XAMG_b200_set_device before init
     bool ready = false;
 

@@ -111,18 +111,17 @@ struct RedArgs {
 // [w*32/VK, (w+1)*32/VK), and a canonical butterfly offset `off` (a multiple
 // of VK, since off >= NV >= VK) is the physical offset off/VK, so every sum is
 // formed from the same operands in the same order as with VK = 1.
-template <typename T, int NV, int NRED, int VK, class Fin>
-__device__ __forceinline__ void canon_finish(T (&acc)[VK][NRED], const RedArgs &ra,
-                                             const Fin &fin) {
+//
+// canon_partial: the block's sum of canonical block cb's accumulators into
+// part[cb] (called by every thread; zeroes acc). A physical block may run
+// several canonical blocks one after the other.
+template <typename T, int NV, int NRED, int VK>
+__device__ __forceinline__ void canon_partial(T (&acc)[VK][NRED], const RedArgs &ra, uint32_t cb) {
     constexpr int NT = CT / VK;   // physical threads of the block
-    constexpr int NW = NT / 32;   // physical warps
     constexpr int SUB = 32 / VK;  // physical threads of one canonical warp
     constexpr int G = NV / VK;    // physical threads of one row slot
     __shared__ T wsum[8 * NV * NRED];
-    __shared__ T sums[NV * NRED];
-    __shared__ int is_last;
     T *part = (T *)ra.part;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int cw = threadIdx.x / SUB, cl = threadIdx.x % SUB;  // canonical lane = cl*VK + v
 #pragma unroll
     for (int v = 0; v < VK; ++v) {
@@ -132,6 +131,7 @@ __device__ __forceinline__ void canon_finish(T (&acc)[VK][NRED], const RedArgs &
 #pragma unroll
             for (int off = 16; off >= NV; off >>= 1) s = add(s, shfl_xor(s, off / VK));
             if (cl < G) wsum[(cw * NV + cl * VK + v) * NRED + r] = s;
+            acc[v][r] = T(0);
         }
     }
     __syncthreads();
@@ -139,8 +139,21 @@ __device__ __forceinline__ void canon_finish(T (&acc)[VK][NRED], const RedArgs &
         T s = wsum[o];
 #pragma unroll
         for (int w = 1; w < 8; ++w) s = add(s, wsum[w * NV * NRED + o]);
-        part[(size_t)blockIdx.x * NV * NRED + o] = s;
+        part[(size_t)cb * NV * NRED + o] = s;
     }
+    __syncthreads();  // wsum is free for the next canonical block
+}
+
+// canon_final: after all of a launch's partials are written, the last
+// physical block to arrive sums the B partials (lane l sums l, l+32, ...,
+// then a full butterfly) and calls fin(k, sums of k).
+template <typename T, int NV, int NRED, int NT, class Fin>
+__device__ __forceinline__ void canon_final(const RedArgs &ra, uint32_t B, const Fin &fin) {
+    constexpr int NW = NT / 32;
+    __shared__ T sums[NV * NRED];
+    __shared__ int is_last;
+    const T *part = (const T *)ra.part;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -152,7 +165,7 @@ __device__ __forceinline__ void canon_finish(T (&acc)[VK][NRED], const RedArgs &
     __threadfence();
     for (int o = warp; o < NV * NRED; o += NW) {
         T a = T(0);
-        for (unsigned bb = lane; bb < gridDim.x; bb += 32)
+        for (unsigned bb = lane; bb < B; bb += 32)
             a = add(a, ld_cg(&part[(size_t)bb * NV * NRED + o]));
 #pragma unroll
         for (int off = 16; off >= 1; off >>= 1) a = add(a, shfl_xor(a, off));
@@ -163,9 +176,11 @@ __device__ __forceinline__ void canon_finish(T (&acc)[VK][NRED], const RedArgs &
     for (int kk = threadIdx.x; kk < NV; kk += NT) fin(kk, &sums[kk * NRED]);
 }
 
+// One canonical block per physical block (256 threads).
 template <typename T, int NV, int NRED, class Fin>
 __device__ __forceinline__ void canon_finish(T (&acc)[NRED], const RedArgs &ra, const Fin &fin) {
-    canon_finish<T, NV, NRED, 1>(reinterpret_cast<T(&)[1][NRED]>(acc), ra, fin);
+    canon_partial<T, NV, NRED, 1>(reinterpret_cast<T(&)[1][NRED]>(acc), ra, blockIdx.x);
+    canon_final<T, NV, NRED, CT>(ra, gridDim.x, fin);
 }
 
 // ---------------------------------------------------------------------------
@@ -365,10 +380,14 @@ __device__ __forceinline__ uint32_t stage_shift(const T *arr, uint32_t j0) {
 // tiles with more entries read global memory directly.
 // CT/VK threads; thread p carries row slot p/(NV/VK) and right-hand sides
 // k0 = (p % (NV/VK))*VK .. k0+VK-1 (x aligned to VK elements).
+// Tiles are dealt round-robin to B canonical blocks (tile t to block t % B);
+// physical block p runs canonical blocks p, p + gridDim.x, ... in turn, so a
+// grid of the blocks that fit the GPU at once covers any B. Without dot
+// products B is simply the grid size.
 template <typename F, typename FX, typename I, int NV, int VK, int NRED, class Epi>
 __global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
     k_spmv(CsrArgs<F> A, const FX *__restrict__ x, Epi epi, RedArgs ra, uint32_t cap,
-           uint32_t nbuf) {
+           uint32_t nbuf, uint32_t B) {
     constexpr int G = NV / VK;
     constexpr int R = CT / NV;
     constexpr int NR = NRED > 0 ? NRED : 1;
@@ -384,6 +403,12 @@ __global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
     const uint64_t n = A.n;
     const uint64_t nnz = n ? row[n] : 0;
     const uint64_t ntiles = (n + R - 1) / R;
+    // tile after t in this physical block's sequence (ntiles: none)
+    auto next_tile = [&](uint64_t t) -> uint64_t {
+        if (t + B < ntiles) return t + B;
+        const uint64_t c = t % B + gridDim.x;
+        return c < B ? c : ntiles;
+    };
     F acc[VK][NR];
 #pragma unroll
     for (int v = 0; v < VK; ++v)
@@ -420,12 +445,13 @@ __global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
     };
     if (threadIdx.x == 0) issue(blockIdx.x);
 
-    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    for (uint64_t tile = blockIdx.x; tile < ntiles;) {
+        const uint64_t tnext = next_tile(tile);
         const uint64_t r0 = tile * R;
         const uint64_t r1 = r0 + R < n ? r0 + R : n;
         const uint32_t tj0 = __ldg(&row[r0]), tj1 = __ldg(&row[r1]);
         const bool staged = tj1 - tj0 <= CAP;
-        if (nbuf == 2 && threadIdx.x == 0) issue(tile + gridDim.x);
+        if (nbuf == 2 && threadIdx.x == 0) issue(tnext);
         const F *sv = nullptr;
         const I *sc = nullptr;
         if (staged) {
@@ -450,7 +476,11 @@ __global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
             for (int v = 0; v < VK; ++v) epi.store(i, k0 + v, y[v], acc[v]);
         }
         __syncthreads();  // every reader is done with this tile's buffer
-        if (nbuf == 1 && threadIdx.x == 0) issue(tile + gridDim.x);
+        if (nbuf == 1 && threadIdx.x == 0) issue(tnext);
+        if constexpr (NRED > 0)
+            if (tnext == ntiles || tnext % B != tile % B)
+                canon_partial<F, NV, NRED, VK>(acc, ra, (uint32_t)(tile % B));
+        tile = tnext;
     }
     if (timed_out) {
         atomicOr(ra.flag, 1u);
@@ -458,7 +488,7 @@ __global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
         if (threadIdx.x == 0)
             for (uint32_t u = n_used; u < n_issued; ++u) mbar_wait(&mbar[u % nbuf], (u / nbuf) & 1u);
     }
-    if constexpr (NRED > 0) canon_finish<F, NV, NRED, VK>(acc, ra, epi);
+    if constexpr (NRED > 0) canon_final<F, NV, NRED, CT / VK>(ra, B, epi);
 }
 
 // Bounded-wait check: one block waits on an mbarrier that nothing arrives

@@ -26,6 +26,7 @@ void Ctx::init() {
                                        (e != cudaSuccess ? cudaGetErrorString(e) : "0 devices"));
     if (device_request >= 0) XG_CUDA(cudaSetDevice(device_request));
     XG_CUDA(cudaGetDevice(&device));
+    XG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     XG_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     red_part.alloc((size_t)k::BMAX * 32 * 3 * sizeof(double));
     red_ticket.alloc(sizeof(unsigned) * 4);

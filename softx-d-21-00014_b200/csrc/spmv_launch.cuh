@@ -1,0 +1,154 @@
+// Launch helpers of the CSR kernels, shared by the ops_spmv*.cu files:
+// runtime (nv, column width) -> template instantiation of k_spmv with the
+// matching epilogue.
+#pragma once
+
+#include <algorithm>
+#include <map>
+#include <tuple>
+#include <type_traits>
+
+#include "ops.h"
+
+namespace xg {
+namespace ops {
+
+template <int V>
+using NVc = std::integral_constant<int, V>;
+
+template <class Fn>
+static void dispatch_nv(int nv, Fn &&fn) {
+    switch (nv) {
+    case 1: fn(NVc<1>()); break;
+    case 2: fn(NVc<2>()); break;
+    case 4: fn(NVc<4>()); break;
+    case 8: fn(NVc<8>()); break;
+    case 16: fn(NVc<16>()); break;
+    case 32: fn(NVc<32>()); break;
+    default: throw Error(XAMG_ERR_INVALID_ARG, "nv must be one of 1,2,4,8,16,32");
+    }
+}
+
+template <class Fn>
+static void dispatch_col(int cb, Fn &&fn) {
+    switch (cb) {
+    case 1: fn((uint8_t *)nullptr); break;
+    case 2: fn((uint16_t *)nullptr); break;
+    case 4: fn((uint32_t *)nullptr); break;
+    case -2: fn((int16_t *)nullptr); break;
+    default: throw Error(XAMG_ERR_INVALID_ARG, "column width must be 1, 2, 4 or -2 bytes");
+    }
+}
+
+// Largest tile entry count for nv: known from the upload for library-owned
+// matrices; for caller-owned device descriptors computed once on the device
+// and remembered per (row pointer, rows). A stale value can only change which
+// tiles are staged, never a result.
+static uint32_t tile_max(const DCsr &A, int nv, cudaStream_t s) {
+    int l = 0;
+    while ((1 << l) < nv) ++l;
+    if (A.tile_max[l] || A.nnz == 0) return A.tile_max[l];
+    static std::map<std::tuple<const void *, uint64_t, int>, uint32_t> cache;
+    auto key = std::make_tuple((const void *)A.row.p, A.nrows, l);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    const uint64_t R = (uint64_t)k::CT >> l;
+    const uint64_t ntiles = (A.nrows + R - 1) / R;
+    unsigned *d = ctx().red_ticket.as<unsigned>() + 1;
+    XG_CUDA(cudaMemsetAsync(d, 0, sizeof(unsigned), s));
+    k::k_tile_max<<<(unsigned)((ntiles + 255) / 256), 256, 0, s>>>(A.row.as<uint32_t>(), A.nrows,
+                                                                     R, d);
+    XG_CUDA(cudaGetLastError());
+    unsigned h = 0;
+    XG_CUDA(cudaMemcpyAsync(&h, d, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    XG_CUDA(cudaStreamSynchronize(s));
+    cache[key] = h;
+    return h;
+}
+
+// Staging buffers: one buffer holds cap entries of values and columns (plus
+// alignment slack); two buffers (the copy of the next tile overlapping the
+// current one) while they fit in 48 KB, at least four blocks per SM; else one
+// buffer of up to 96 KB.
+template <typename F, typename I>
+static uint32_t stage_buffer_bytes(uint32_t cap) {
+    auto r16 = [](uint64_t b) { return (uint32_t)((b + 15) & ~(uint64_t)15); };
+    return r16((uint64_t)cap * sizeof(F) + 32) + r16((uint64_t)cap * sizeof(I) + 32);
+}
+
+// Grid: as many blocks as fit the GPU at once (one wave). With dot products
+// the tiles still go to the canonical B = min(ntiles, 1184) blocks, which the
+// grid's blocks run in turn; without, the grid's blocks take the tiles.
+template <typename F, typename FX, typename I, int NV, int VK, int NRED, class Epi>
+static void launch_vk(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s) {
+    constexpr uint32_t LIMIT1 = (96u * 1024u - 64u) / (uint32_t)(sizeof(F) + sizeof(I));
+    const uint32_t tm = tile_max(A, NV, s);
+    uint32_t cap = tm, nbuf = 2;
+    if (2 * stage_buffer_bytes<F, I>(tm) > 48u * 1024u) {
+        nbuf = 1;
+        cap = std::min(tm, LIMIT1);
+    }
+    const size_t smem = (size_t)nbuf * stage_buffer_bytes<F, I>(cap);
+    auto kern = k::k_spmv<F, FX, I, NV, VK, NRED, Epi>;
+    static bool big_smem = false;  // one flag per instantiation
+    if (smem > 48u * 1024u && !big_smem) {
+        XG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)stage_buffer_bytes<F, I>(LIMIT1)));
+        big_smem = true;
+    }
+    static std::map<size_t, int> resident;  // per instantiation: blocks per SM by smem
+    auto it = resident.find(smem);
+    if (it == resident.end()) {
+        int nb = 0;
+        XG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, k::CT / VK, smem));
+        it = resident.emplace(smem, std::max(nb, 1)).first;
+    }
+    const uint64_t R = k::CT / NV;
+    const uint64_t ntiles = (A.nrows + R - 1) / R;
+    const uint64_t wave = (uint64_t)it->second * (uint64_t)ctx().sms;
+    const uint32_t B = NRED > 0 ? (uint32_t)k::canon_blocks(A.nrows, NV)
+                                : (uint32_t)std::min<uint64_t>(ntiles, wave);
+    const uint32_t P = (uint32_t)std::min<uint64_t>(B, wave);
+    kern<<<P, k::CT / VK, smem, s>>>(A.args<F>(), x, epi, ctx().red(), cap, nbuf, B);
+    XG_CUDA(cudaGetLastError());
+    ++g_kernel_launches;
+}
+
+// Vector loads of x need x aligned to VK elements; library vectors always are
+// (cudaMalloc). The entry points that take a caller's x (CALLER_X) fall back
+// to one right-hand side per thread for an x that is not (same results, same
+// reduction order).
+template <typename F, typename FX, typename I, int NV, int NRED, bool CALLER_X = false,
+          class Epi>
+static void launch(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s) {
+    if (A.nrows == 0) return;
+    constexpr int VK = k::spmv_vk<FX, NV>();
+    constexpr uintptr_t ALIGN = VK * sizeof(FX);
+    if (VK == 1 || (uintptr_t)x % ALIGN == 0) {
+        launch_vk<F, FX, I, NV, VK, NRED>(A, x, epi, s);
+    } else if constexpr (CALLER_X) {
+        launch_vk<F, FX, I, NV, 1, NRED>(A, x, epi, s);
+    } else {
+        throw Error(XAMG_ERR_INTERNAL, "library vector not aligned for the SpMV gather");
+    }
+}
+
+template <typename F, int NV, int NRED, class Epi>
+static void launch_rows(uint64_t n, const Epi &epi, cudaStream_t s) {
+    if (n == 0) return;
+    const int B = k::canon_blocks(n, NV);
+    k::k_rows<F, NV, NRED, Epi><<<B, k::CT, 0, s>>>(n, epi, ctx().red());
+    XG_CUDA(cudaGetLastError());
+    ++g_kernel_launches;
+}
+
+#define XG_DISPATCH(A, nv, ...)                                             \
+    dispatch_nv(nv, [&](auto nvc) {                                         \
+        constexpr int NV = decltype(nvc)::value;                            \
+        dispatch_col((A).col_bytes, [&](auto ip) {                          \
+            using I = std::remove_pointer_t<decltype(ip)>;                  \
+            __VA_ARGS__;                                                    \
+        });                                                                 \
+    })
+}  // namespace ops
+}  // namespace xg
