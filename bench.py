@@ -17,8 +17,9 @@ right-hand-side block on its own GPU (weak scaling, no data-path
 collective); times are the maximum over ranks.
 
 --impl reference times the CPU oracle (the restatement of XAMG's FP64 CPU
-solve; the reference's own build needs MPI, hypre, argsparser and yaml-cpp)
-on a bounded sample of the same solve.
+solve, its SpMV rows threaded over the host cores; the reference's own build
+needs MPI, hypre, argsparser and yaml-cpp) on a bounded sample of the same
+solve.
 """
 import argparse
 import json
@@ -95,7 +96,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -182,8 +183,11 @@ def run_ours(args, w):
     setup_s = time.time() - t0
     chosen = "chosen" if "chosen" in solvers else "fp64"
 
+    # pinned host buffers for the end-to-end arm
+    bh = torch.from_numpy(b).pin_memory()
+    xh_pin = torch.empty(n * nv, dtype=torch.float64).pin_memory()
+
     def timed(S, K, e2e=False):
-        xh = np.empty(n * nv)
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         barrier(ws)
@@ -193,17 +197,20 @@ def run_ours(args, w):
             ev0.record(stream)
             for _ in range(K):
                 if e2e:
-                    bv.upload(b)
+                    X.call("XAMG_vector_upload_d", bh.data_ptr(), n, 0, nv, bv.h)
                 xv.set(0.0)
                 S.solve()
                 if e2e:
-                    X.call("XAMG_vector_download_d", xh.ctypes.data, n, 0, nv, xv.h)
+                    X.call("XAMG_vector_download_d", xh_pin.data_ptr(), n, 0, nv, xv.h)
             ev1.record(stream)
         ev1.synchronize()
         torch.cuda.synchronize()
         barrier(ws)
         ms = ev0.elapsed_time(ev1)
-        return max_over_ranks(ms, ws), X.kernel_launches() - k0, xh
+        return max_over_ranks(ms, ws), X.kernel_launches() - k0, xh_pin.numpy().copy()
+
+    if args.roofline_only:
+        return roofline(X, torch, stream, solvers[chosen], n, nv, args, reps=args.steps)
 
     res = {}
     for name, S in solvers.items():
@@ -223,32 +230,8 @@ def run_ours(args, w):
     Xs, Bs = xh.reshape(n, nv), b.reshape(n, nv)
     true_rel = (np.linalg.norm(Bs - A @ Xs, axis=0) / np.linalg.norm(Bs, axis=0)).max()
 
-    # roofline of the dominant kernel: fine-level SpMV (f64, nv RHS)
-    A0 = S.level_csr(0, 0)
-    xd = torch.empty(n * nv, dtype=torch.float64, device="cuda").uniform_(-1, 1)
-    yd = torch.empty(n * nv, dtype=torch.float64, device="cuda")
-    reps = 50
-    torch.cuda.synchronize()
-    for _ in range(3):
-        X.call("XAMG_b200_spmv", A0, xd.data_ptr(), yd.data_ptr(), nv, 0, X.stream())
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with torch.cuda.stream(stream):
-        e0.record(stream)
-        for _ in range(reps):
-            X.call("XAMG_b200_spmv", A0, xd.data_ptr(), yd.data_ptr(), nv, 0, X.stream())
-        e1.record(stream)
-    e1.synchronize()
-    spmv_ms = e0.elapsed_time(e1) / reps
-    nnz = A0.nnz
-    alg_bytes = nnz * (8 + abs(A0.col_bytes)) + (n + 1) * 4 + 2 * n * nv * 8
-    achieved = alg_bytes / (spmv_ms * 1e-3) / 1e9
-    peak, peak_kind = peaks()
-    traffic = None
-    tfile = os.path.join(ROOT, "profiles", "spmv_traffic.json")
-    if os.path.exists(tfile):
-        t = json.load(open(tfile)).get(f"{args.workload}_nv{nv}")
-        if t:
-            traffic = t["dram_bytes_per_launch"]
+    rf = roofline(X, torch, stream, S, n, nv, args)
+    rf64 = roofline(X, torch, stream, S, n, nv, args, which=0)
 
     total_rhs = args.steps * nv * ws
     out = {
@@ -271,11 +254,8 @@ def run_ours(args, w):
         "e2e": {"value": ms_e2e / total_rhs * ws, "unit": "ms/RHS",
                 "h2d_bytes_per_step": n * nv * 8, "d2h_bytes_per_step": n * nv * 8},
         "gpu_launches": int(res[chosen]["launches"]),
-        "roofline": {"bound": "hbm", "kernel": "k_spmv<double> fine level",
-                     "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": traffic, "algorithmic_bytes": int(alg_bytes),
-                     "ms_per_launch": spmv_ms},
+        "roofline": rf,
+        "roofline_krylov_spmv": rf64,
         "clocks": res[chosen]["clocks"],
         "setup_s": setup_s,
     }
@@ -288,40 +268,99 @@ def run_ours(args, w):
     return out if rank == 0 else None
 
 
-def cpu_baseline(X, S, w, row, col, val, b, iters_full, args, threads=1):
-    """The oracle on the host: a bounded sample of the same plain-FP64 solve
-    (a few outer iterations), scaled to the full iteration count."""
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import oracle_py as O
-    nv = w["nv"]
-    params = params_for(w, False)
-    sample_iters = args.cpu_iters
-    p = json.loads(json.dumps(params))
-    p["solver"]["max_iters"] = sample_iters
-    p["solver"]["rel_tolerance"] = 0.0
-    sysm = O.System(nv)
-    sysm.set_params(p)
-    if w["smoother"] is None:
-        sysm.add_level(row, col, val)
-    else:
-        # the same hierarchy the GPU solver uses (the oracle applies XAMG's
-        # parse and setup on it)
-        for lv in S.hierarchy():
-            sysm.add_level(*lv["A"], lv["min_eig"], lv["max_eig"])
-            if lv["P"] is not None:
-                sysm.add_interp(*lv["P"])
-    sysm.setup()
-    t0 = time.perf_counter()
-    _, st = sysm.solve(b)
-    dt = time.perf_counter() - t0
-    per_iter = dt / max(1, st["iters"])
-    ms_rhs = per_iter * iters_full * 1e3 / nv
-    return {"value": ms_rhs, "unit": "ms/RHS", "cores": threads, "kind": "port",
-            "sample": f"{st['iters']} outer iterations of the plain-FP64 solve "
+def roofline(X, torch, stream, S, n, nv, args, which=3, reps=50):
+    """The finest level's SpMV y = A x through XAMG_b200_spmv on the solver's
+    own uploaded matrix: which=3 the operator the multigrid cycle applies (the
+    FP32 copy in the chosen form: the smoother and residual SpMVs, the largest
+    share of the solve), which=0 the Krylov level's FP64 matrix. Algorithmic
+    bytes per launch: values and narrowed columns once, row pointers, x read
+    and y written once (x's reuse across rows is served by the caches)."""
+    A0 = S.level_csr(0, which)
+    esz = 4 if A0.val_f32 else 8
+    dt = torch.float32 if A0.val_f32 else torch.float64
+    xd = torch.empty(n * nv, dtype=dt, device="cuda").uniform_(-1, 1)
+    yd = torch.empty(n * nv, dtype=dt, device="cuda")
+    torch.cuda.synchronize()
+    for _ in range(3):
+        X.call("XAMG_b200_spmv", A0, xd.data_ptr(), yd.data_ptr(), nv, 0, X.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(reps):
+            X.call("XAMG_b200_spmv", A0, xd.data_ptr(), yd.data_ptr(), nv, 0, X.stream())
+        e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    alg = A0.nnz * (esz + abs(A0.col_bytes)) + (n + 1) * 4 + 2 * n * nv * esz
+    achieved = alg / (ms * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+    kname = f"k_spmv<{'float' if esz == 4 else 'double'}> level 0, EStore, nv={nv}, " \
+            f"col_bytes={A0.col_bytes}"
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "spmv_traffic.json")
+    if os.path.exists(tfile):
+        t = json.load(open(tfile)).get(f"{args.workload}_which{which}_nv{nv}")
+        if t:
+            traffic = t["dram_bytes_per_launch"]
+    return {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
+            "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+            "traffic": traffic, "algorithmic_bytes": int(alg), "ms_per_launch": ms,
+            "launches_timed": reps}
+
+
+class OracleArm:
+    """The oracle on the host (the restatement of XAMG's FP64 CPU solve): the
+    same plain-FP64 solve on the same hierarchy, cut to a bounded sample of
+    `sample_iters` outer iterations per step."""
+
+    def __init__(self, S, w, row, col, val, b, sample_iters):
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_py as O
+        self.nv = w["nv"]
+        p = json.loads(json.dumps(params_for(w, False)))
+        p["solver"]["max_iters"] = sample_iters
+        p["solver"]["rel_tolerance"] = 0.0
+        self.sysm = O.System(self.nv)
+        self.sysm.set_params(p)
+        if w["smoother"] is None:
+            self.sysm.add_level(row, col, val)
+        else:
+            # the hierarchy the GPU solver uses (the oracle applies XAMG's
+            # parse and setup on it)
+            for lv in S.hierarchy():
+                self.sysm.add_level(*lv["A"], lv["min_eig"], lv["max_eig"])
+                if lv["P"] is not None:
+                    self.sysm.add_interp(*lv["P"])
+        self.sysm.setup()
+        self.b = b
+        self.cores = O.threads()
+
+    def step(self):
+        """Seconds per outer iteration of one sampled solve."""
+        t0 = time.perf_counter()
+        _, st = self.sysm.solve(self.b)
+        dt = time.perf_counter() - t0
+        self.last = (dt, st["iters"])
+        return dt / max(1, st["iters"])
+
+
+def cpu_baseline(X, S, w, row, col, val, b, iters_full, args):
+    """A bounded sample of the plain-FP64 solve on the oracle, scaled to the
+    full iteration count."""
+    arm = OracleArm(S, w, row, col, val, b, args.cpu_iters)
+    per_iter = arm.step()
+    dt, it = arm.last
+    ms_rhs = per_iter * iters_full * 1e3 / w["nv"]
+    return {"value": ms_rhs, "unit": "ms/RHS", "cores": arm.cores, "kind": "port",
+            "sample": f"{it} outer iterations of the plain-FP64 solve "
                       f"({dt:.1f} s), scaled to the GPU's {iters_full} iterations"}
 
 
 def run_reference(args, w):
+    """CPU arm: the oracle's plain-FP64 solve (C++, SpMV rows on all host
+    threads), each step one sampled outer iteration of the full-size solve
+    scaled to the iteration count the solve needs; one untimed warm-up step,
+    median of K."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return None
@@ -337,18 +376,23 @@ def run_reference(args, w):
     S = X.Solver(M, X.Params(params_for(w, False)), xv, bv)
     S.solve()
     iters = S.stats()["iters"]
-    vals = []
-    for _ in range(args.steps):
-        vals.append(cpu_baseline(X, S, w, row, col, val, b, iters, args)["value"])
+    arm = OracleArm(S, w, row, col, val, b, args.cpu_iters)
+    for _ in range(min(args.warmup, 1)):
+        arm.step()
+    vals = [arm.step() * iters * 1e3 / w["nv"] for _ in range(args.steps)]
     v = float(np.median(vals))
-    cb = cpu_baseline(X, S, w, row, col, val, b, iters, args)
+    dt, it = arm.last
+    cb = {"value": v, "unit": "ms/RHS", "cores": arm.cores, "kind": "port",
+          "sample": f"per step {it} outer iteration(s) of the plain-FP64 solve ({dt:.1f} s), "
+                    f"scaled to the {iters} iterations of the full solve; median of "
+                    f"{args.steps} steps"}
     return {"impl": "reference",
             "metric": "ms/RHS to 1e-8 residual: chosen vs plain FP64 on 1 B200; SpMV % of HBM BW",
             "value": v, "unit": "ms/RHS", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "warmup": args.warmup, "ms_per_step": v * w["nv"], "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": w["desc"], "rows": n, "nv": w["nv"]},
-            "cpu_baseline": dict(cb, value=v),
+            "cpu_baseline": cb,
             "e2e": {"value": v, "unit": "ms/RHS", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
 
@@ -356,13 +400,16 @@ def run_reference(args, w):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="amg27", choices=sorted(WORKLOADS))
     ap.add_argument("--grid", type=int, default=None, help="override the grid edge")
     ap.add_argument("--cpu-iters", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--roofline-only", action="store_true",
+                    help="set up, then time only the level-0 SpMV (--steps launches): "
+                         "the command to profile that kernel")
     args = ap.parse_args()
     w = dict(WORKLOADS[args.workload])
     if args.grid:

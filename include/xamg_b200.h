@@ -125,8 +125,10 @@ int XAMG_b200_solver_stats(size_t sid, int *iters, int *conv, double *abs_res, d
  * (1 when the solver has no multigrid). */
 int XAMG_b200_solver_nlevels(size_t sid);
 
-/* Shape of level matrix `which` (0 = A, 1 = R, 2 = P) as uploaded: sizes,
- * narrowed column width, value type, XAMG hash, eigenvalue estimates. */
+/* Shape of level matrix `which` (0 = A, 1 = R, 2 = P, 3 = the operator the
+ * multigrid cycle applies on the level: A, or on level 0 the FP32 copy when
+ * gpu_precond_f32 is set) as uploaded: sizes, narrowed column width, value
+ * type, XAMG hash, eigenvalue estimates. */
 int XAMG_b200_solver_level_info(size_t sid, int level, int which, uint64_t *nrows,
                                 uint64_t *ncols, uint64_t *nnz, int *col_bytes, int *val_f32,
                                 uint16_t *hash, double *min_eig, double *max_eig);
@@ -142,7 +144,7 @@ int XAMG_b200_solver_level_download(size_t sid, int level, int which, uint32_t *
 int XAMG_b200_solver_hierarchy_export(size_t sid, int level, int which, uint32_t *row,
                                       uint32_t *col, double *val);
 
-/* Device pointers of an uploaded level matrix (which = 0 A, 1 R, 2 P), for
+/* Device pointers of an uploaded level matrix (which as above), for
  * running the kernel entry points on the solver's own data (no counterpart). */
 int XAMG_b200_solver_level_csr(size_t sid, int level, int which, XAMG_b200_csr *out);
 

@@ -20,6 +20,9 @@
 // reference obtains it from hypre 2.20.0, which is not available); the oracle
 // restates everything XAMG does after hypre returns.
 
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 #include <algorithm>
 #include <cassert>
 #include <cmath>
@@ -914,6 +917,9 @@ void csr_Ax_y(const Csr &m, const Vec &x, Vec &y) {
     const T *xp = x.p<T>();
     T *yp = y.p<T>();
     const T *v = m.val<T>();
+    // rows are independent (each is summed sequentially by one thread), so
+    // the threads change no result
+#pragma omp parallel for schedule(static)
     for (uint64_t i = 0; i < m.nrows; ++i) {
         uint64_t rs = (m.indexed ? m.row_ind[i] : i) * NV;
         for (int k = 0; k < NV; ++k) yp[rs + k] = 0.0;
@@ -938,6 +944,7 @@ void csr_Axpy(const Csr &m, const Vec &x, Vec &y, uint64_t m_offset = 0) {
     const T *xp = x.p<T>();
     T *yp = y.p<T>();
     const T *v = m.val<T>();
+#pragma omp parallel for schedule(static)
     for (uint64_t i = 0; i < m.nrows; ++i) {
         uint64_t rs = ((m.indexed ? m.row_ind[i] : i) + m_offset) * NV;
         for (uint64_t j = m.row[i]; j < m.row[i + 1]; ++j) {
@@ -1926,6 +1933,15 @@ using namespace orc;
 extern "C" {
 
 int or_version() { return 1; }
+
+// Threads the SpMV row loops use (OMP_NUM_THREADS, default: all cores).
+int or_threads() {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
 
 void or_set_reduction(int mode, int ncores) {
     g_red.mode = mode;

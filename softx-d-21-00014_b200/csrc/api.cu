@@ -791,8 +791,9 @@ static const DCsr &level_matrix(size_t sid, int level, int which) {
         return *so.sh->A;
     }
     XG_REQUIRE(level >= 0 && level < (int)mg->L.size(), XAMG_ERR_INVALID_ARG, "bad level");
-    XG_REQUIRE(which >= 0 && which <= 2, XAMG_ERR_INVALID_ARG, "which must be 0, 1 or 2");
+    XG_REQUIRE(which >= 0 && which <= 3, XAMG_ERR_INVALID_ARG, "which must be 0, 1, 2 or 3");
     if (which == 0) return level == 0 ? *so.sh->A : mg->L[level].A;
+    if (which == 3) return level == 0 && !mg->full32 ? *so.sh->A : mg->L[level].A;
     XG_REQUIRE(level + 1 < (int)mg->L.size(), XAMG_ERR_INVALID_ARG, "coarsest level has no R/P");
     return which == 1 ? mg->L[level].R : mg->L[level].P;
 }

@@ -219,17 +219,21 @@ __device__ __forceinline__ uint64_t col_at(I c, uint64_t i) {
         return (uint64_t)c;
 }
 
-// Right-hand sides one SpMV thread carries: x[c*NV + k0 .. k0+VK-1] is one
-// aligned load of at most 16 bytes, so a warp issues 1/VK of the
+// Right-hand sides one SpMV thread carries: x[c*NV + k0 .. k0+VK-1] is
+// loaded with 16-byte (or 8-byte) vector loads, so a warp issues 1/VK of the
 // shared-memory reads of (column, value) and of the gather instructions that
 // a thread per right-hand side would. The canonical order does not change
 // (canon_finish).
-#ifndef XG_SPMV_VK
-#define XG_SPMV_VK 2
+#ifndef XG_SPMV_VK64
+#define XG_SPMV_VK64 2  // FP64 x
 #endif
+#ifndef XG_SPMV_VK32
+#define XG_SPMV_VK32 4  // FP32 x
+#endif
+// (The launcher may also pick 4 for FP64 x on short rows.)
 template <typename FX, int NV>
 __host__ __device__ constexpr int spmv_vk() {
-    constexpr int w = 16 / (int)sizeof(FX) < XG_SPMV_VK ? 16 / (int)sizeof(FX) : XG_SPMV_VK;
+    constexpr int w = sizeof(FX) == 8 ? XG_SPMV_VK64 : XG_SPMV_VK32;
     return NV < w ? NV : w;
 }
 
@@ -263,11 +267,10 @@ __device__ __forceinline__ void ld_x(const FX *p, FX (&o)[VK]) {
 // Row accumulation, entry by entry in row order (the loop is unrolled so that
 // gathers of later entries can issue before earlier sums complete; the
 // additions stay in order). cl/vl point at the row's first entry.
-// Resident blocks the register budget allows: at most 64 registers a thread
-// (a block of 256 threads also needs a 40 KB staging pair, so no more than
-// five fit an SM anyway).
+// Resident blocks the register budget is set for: 1024 threads an SM at 64
+// registers a thread, whatever the block size.
 template <int VK>
-constexpr int spmv_min_blocks() { return VK == 1 ? 4 : 8; }
+constexpr int spmv_min_blocks() { return 4 * VK; }
 
 template <typename F, typename FX, typename I, int NV, int VK>
 __device__ __forceinline__ void row_sum(F (&y)[VK], uint32_t len, uint64_t i, int k0, const I *cl,

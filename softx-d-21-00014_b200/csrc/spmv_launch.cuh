@@ -118,13 +118,20 @@ static void launch_vk(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s
 // (cudaMalloc). The entry points that take a caller's x (CALLER_X) fall back
 // to one right-hand side per thread for an x that is not (same results, same
 // reduction order).
+// FP64 x on short rows (fewer than 16 entries on average: 7-point stencils
+// and the like) takes four right-hand sides per thread: the staging buffers
+// are small enough for sixteen 64-thread blocks an SM, and the wider gathers
+// win; longer rows keep two.
 template <typename F, typename FX, typename I, int NV, int NRED, bool CALLER_X = false,
           class Epi>
 static void launch(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s) {
     if (A.nrows == 0) return;
     constexpr int VK = k::spmv_vk<FX, NV>();
     constexpr uintptr_t ALIGN = VK * sizeof(FX);
-    if (VK == 1 || (uintptr_t)x % ALIGN == 0) {
+    constexpr bool SHORT4 = sizeof(FX) == 8 && VK == 2 && NV >= 4 && NRED <= 1;
+    if (SHORT4 && A.nnz < 16 * A.nrows && (uintptr_t)x % (4 * sizeof(FX)) == 0) {
+        if constexpr (SHORT4) launch_vk<F, FX, I, NV, 4, NRED>(A, x, epi, s);
+    } else if (VK == 1 || (uintptr_t)x % ALIGN == 0) {
         launch_vk<F, FX, I, NV, VK, NRED>(A, x, epi, s);
     } else if constexpr (CALLER_X) {
         launch_vk<F, FX, I, NV, 1, NRED>(A, x, epi, s);

@@ -25,6 +25,11 @@ def build():
     subprocess.check_call(["make", "-s", "-C", ORACLE_DIR])
 
 
+def threads():
+    """Threads the oracle's SpMV loops run on (OMP_NUM_THREADS or all cores)."""
+    return int(lib().or_threads())
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -54,6 +59,7 @@ def lib():
         L.or_group1.argtypes = [C.c_uint64, C.c_int, f64p, f64p, f64p, f64p, f64p]
         L.or_group2.argtypes = [C.c_uint64, C.c_int, f64p, f64p, f64p, f64p, f64p]
         L.or_group4.argtypes = [C.c_uint64, C.c_int, f64p, f64p, f64p, f64p, f64p, f64p]
+        L.or_threads.restype = C.c_int
         L.or_generate_cube.restype = C.c_uint64
         L.or_generate_cube.argtypes = [C.c_uint64] * 3 + [u32p, u32p, f64p]
         L.or_sys_create.restype = C.c_void_p
