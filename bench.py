@@ -245,7 +245,7 @@ def run_ours(args, w):
         "data": "synthetic",
         "config": {"workload": w["desc"], "rows": n, "nnz": int(len(col)), "nv": nv,
                    "rhs_per_gpu_per_step": nv, "tolerance": 1e-8,
-                   "l2": "inputs larger than L2 (matrix > 126 MB)" if nnz * 12 > 126e6
+                   "l2": "inputs larger than L2 (matrix > 126 MB)" if len(col) * 12 > 126e6
                    else "L2-resident inputs (no flush)"},
         "iters": {k: v["iters"] for k, v in res.items()},
         "plain_fp64_ms_per_rhs": res["fp64"]["ms"] / total_rhs * ws,
