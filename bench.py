@@ -131,27 +131,17 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
-def dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+from replicas import dist_env, rhs_blocks  # noqa: E402
+import replicas  # noqa: E402
 
 
 def max_over_ranks(v, ws):
-    if ws == 1:
-        return v
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return replicas.max_over_ranks(v) if ws > 1 else v
 
 
 def barrier(ws):
     if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
+        replicas.barrier()
 
 
 def run_ours(args, w):
@@ -170,7 +160,8 @@ def run_ours(args, w):
     row, col, val = make_matrix(X, w)
     n = len(row) - 1
     M = X.Matrix(row, col, val)
-    rng = np.random.default_rng(1000 + rank)
+    # weak scaling: one right-hand-side block per rank, seeded by its index
+    rng = np.random.default_rng(1000 + rhs_blocks(ws, ws, rank)[0])
     b = rng.uniform(-1, 1, n * nv)
     bv, xv = X.Vector(n, nv), X.Vector(n, nv)
     bv.upload(b)
