@@ -260,8 +260,8 @@ def run_ours(args, w):
 
 
 def roofline(X, torch, stream, S, n, nv, args, which=3, reps=50):
-    """The finest level's SpMV y = A x through XAMG_b200_spmv on the solver's
-    own uploaded matrix: which=3 the operator the multigrid cycle applies (the
+    """The finest level's SpMV y = A x through XAMG_b200_solver_level_spmv on
+    the solver's own uploaded matrix, as its solves run it: which=3 the operator the multigrid cycle applies (the
     FP32 copy in the chosen form: the smoother and residual SpMVs, the largest
     share of the solve), which=0 the Krylov level's FP64 matrix. Algorithmic
     bytes per launch: values and narrowed columns once, row pointers, x read
@@ -273,12 +273,12 @@ def roofline(X, torch, stream, S, n, nv, args, which=3, reps=50):
     yd = torch.empty(n * nv, dtype=dt, device="cuda")
     torch.cuda.synchronize()
     for _ in range(3):
-        X.call("XAMG_b200_spmv", A0, xd.data_ptr(), yd.data_ptr(), nv, 0, X.stream())
+        S.level_spmv(0, which, xd.data_ptr(), yd.data_ptr(), nv)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(stream):
         e0.record(stream)
         for _ in range(reps):
-            X.call("XAMG_b200_spmv", A0, xd.data_ptr(), yd.data_ptr(), nv, 0, X.stream())
+            S.level_spmv(0, which, xd.data_ptr(), yd.data_ptr(), nv)
         e1.record(stream)
     e1.synchronize()
     ms = e0.elapsed_time(e1) / reps

@@ -148,6 +148,14 @@ int XAMG_b200_solver_hierarchy_export(size_t sid, int level, int which, uint32_t
  * running the kernel entry points on the solver's own data (no counterpart). */
 int XAMG_b200_solver_level_csr(size_t sid, int level, int which, XAMG_b200_csr *out);
 
+/* y = A x (mode 0) or y += A x (mode 1) with level matrix `which` of a
+ * solver, as its solves run it: on the library's own copy, with the x-staging
+ * plan it has for nv (no counterpart; the kernel-level view of the solver's
+ * SpMV for tests and timing). x and y are device arrays of the level's value
+ * type, nrows x nv and ncols x nv. */
+int XAMG_b200_solver_level_spmv(size_t sid, int level, int which, const void *x, void *y, int nv,
+                                int mode, void *stream);
+
 /* Number of kernels this library has launched since it was loaded (no
  * counterpart; used to account for the device work of a timed region). */
 uint64_t XAMG_b200_kernel_launches(void);

@@ -860,6 +860,19 @@ int XAMG_b200_solver_level_csr(size_t sid, int level, int which, XAMG_b200_csr *
     });
 }
 
+int XAMG_b200_solver_level_spmv(size_t sid, int level, int which, const void *x, void *y, int nv,
+                                int mode, void *stream) {
+    return guarded([&] {
+        check_nv(nv);
+        const DCsr &d = level_matrix(sid, level, which);
+        cudaStream_t s = pick(stream);
+        if (d.f32)
+            ops::spmv<float>(d, (const float *)x, (float *)y, nv, mode == 1, s);
+        else
+            ops::spmv<double>(d, (const double *)x, (double *)y, nv, mode == 1, s);
+    });
+}
+
 uint64_t XAMG_b200_kernel_launches(void) { return g_kernel_launches; }
 
 void *XAMG_b200_stream(void) {

@@ -1,4 +1,4 @@
-// SpMV entry points: y = Ax, y += Ax, and the FP64 -> FP32 restriction.
+// SpMV entry points for FP64: y = Ax, y += Ax; and the bounded-wait check.
 #include "spmv_launch.cuh"
 
 namespace xg {
@@ -20,11 +20,6 @@ void spmv(const DCsr &A, const F *x, F *y, int nv, bool axpy, cudaStream_t s) {
     });
 }
 template void spmv<double>(const DCsr &, const double *, double *, int, bool, cudaStream_t);
-template void spmv<float>(const DCsr &, const float *, float *, int, bool, cudaStream_t);
-
-void spmv_f32_from_f64(const DCsr &A, const double *x, float *y, int nv, cudaStream_t s) {
-    XG_DISPATCH(A, nv, { launch<float, double, I, NV, 0>(A, x, k::EStore<float, NV>{{}, y}, s); });
-}
 
 }  // namespace ops
 }  // namespace xg

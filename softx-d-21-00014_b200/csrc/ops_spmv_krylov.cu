@@ -1,24 +1,9 @@
-// SpMV kernels of the Krylov solvers (residuals, merged BiCGStab groups with
+// SpMV kernels of the Krylov solvers (merged BiCGStab groups with
 // their dot products) and the canonical-order vector reductions.
 #include "spmv_launch.cuh"
 
 namespace xg {
 namespace ops {
-
-template <typename F>
-void residual(const DCsr &A, const F *x, const F *b, F *r, int nv, double *norm_out,
-              cudaStream_t s) {
-    XG_DISPATCH(A, nv, {
-        if (norm_out)
-            launch<F, F, I, NV, 1>(A, x, k::EResid<F, NV, true>{r, b, norm_out}, s);
-        else
-            launch<F, F, I, NV, 0>(A, x, k::EResid<F, NV, false>{r, b, nullptr}, s);
-    });
-}
-template void residual<double>(const DCsr &, const double *, const double *, double *, int,
-                               double *, cudaStream_t);
-template void residual<float>(const DCsr &, const float *, const float *, float *, int, double *,
-                              cudaStream_t);
 
 void group1(const DCsr &A, const double *x, const double *b, double *r0, double *p, double *r,
             double *sc, int nv, cudaStream_t s) {

@@ -343,7 +343,16 @@ struct Chebyshev : public SolverBase {
 template <typename F>
 struct Direct : public SolverBase {
     DevBuf inv;
+    // The explicit inverse is dense (n^2 values, inverse.inl:31-106): refuse
+    // sizes whose inverse would not fit host and device memory comfortably
+    // instead of running out of memory (the hierarchy's coarsest level is
+    // this large when mg_max_levels stops the coarsening early).
+    static constexpr uint64_t MAX_N = 16384;
     void setup_from(const HCsr &hA) {
+        XG_REQUIRE(hA.nrows <= MAX_N, XAMG_ERR_UNSUPPORTED,
+                   "direct solver on " + std::to_string(hA.nrows) +
+                       " rows (at most 16384): coarsen further (mg_max_levels, "
+                       "mg_coarse_matrix_size)");
         if (f32)
             upload(inv, dense_inverse_f32(hA), S());
         else

@@ -82,6 +82,13 @@ static uint32_t stage_buffer_bytes(uint32_t cap) {
 template <typename F, typename FX, typename I, int NV, int VK, int NRED, class Epi>
 static void launch_vk(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s) {
     constexpr uint32_t LIMIT1 = (96u * 1024u - 64u) / (uint32_t)(sizeof(F) + sizeof(I));
+    auto kern = k::k_spmv<F, FX, I, NV, VK, NRED, Epi>;
+    static bool big_smem = false;  // one flag per instantiation
+    if (!big_smem) {
+        XG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)stage_buffer_bytes<F, I>(LIMIT1)));
+        big_smem = true;
+    }
     const uint32_t tm = tile_max(A, NV, s);
     uint32_t cap = tm, nbuf = 2;
     if (2 * stage_buffer_bytes<F, I>(tm) > 48u * 1024u) {
@@ -89,13 +96,6 @@ static void launch_vk(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s
         cap = std::min(tm, LIMIT1);
     }
     const size_t smem = (size_t)nbuf * stage_buffer_bytes<F, I>(cap);
-    auto kern = k::k_spmv<F, FX, I, NV, VK, NRED, Epi>;
-    static bool big_smem = false;  // one flag per instantiation
-    if (smem > 48u * 1024u && !big_smem) {
-        XG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)stage_buffer_bytes<F, I>(LIMIT1)));
-        big_smem = true;
-    }
     static std::map<size_t, int> resident;  // per instantiation: blocks per SM by smem
     auto it = resident.find(smem);
     if (it == resident.end()) {
@@ -128,7 +128,7 @@ static void launch(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s) {
     if (A.nrows == 0) return;
     constexpr int VK = k::spmv_vk<FX, NV>();
     constexpr uintptr_t ALIGN = VK * sizeof(FX);
-    constexpr bool SHORT4 = sizeof(FX) == 8 && VK == 2 && NV >= 4 && NRED <= 1;
+    constexpr bool SHORT4 = sizeof(FX) == 8 && VK == 2 && NV >= 4 && NRED == 0;
     if (SHORT4 && A.nnz < 16 * A.nrows && (uintptr_t)x % (4 * sizeof(FX)) == 0) {
         if constexpr (SHORT4) launch_vk<F, FX, I, NV, 4, NRED>(A, x, epi, s);
     } else if (VK == 1 || (uintptr_t)x % ALIGN == 0) {

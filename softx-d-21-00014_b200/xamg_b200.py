@@ -55,6 +55,7 @@ EXT_SYMBOLS = [
     "XAMG_b200_solver_hierarchy_export", "XAMG_b200_vector_device_ptr",
     "XAMG_b200_solver_level_csr", "XAMG_b200_kernel_launches", "XAMG_b200_stream",
     "XAMG_b200_set_device", "XAMG_b200_dot_noalloc", "XAMG_b200_wait_selftest",
+    "XAMG_b200_solver_level_spmv",
 ]
 
 
@@ -169,6 +170,8 @@ def lib():
         "XAMG_b200_stream": (vp, []),
         "XAMG_b200_set_device": (C.c_int, [C.c_int]),
         "XAMG_b200_wait_selftest": (C.c_int, [C.c_double, C.POINTER(C.c_int)]),
+        "XAMG_b200_solver_level_spmv": (C.c_int, [C.c_size_t, C.c_int, C.c_int, vp, vp, C.c_int,
+                                                  C.c_int, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -395,6 +398,11 @@ class Solver:
         call("XAMG_b200_solver_level_download", self.h, level, which, _ptr(row), _ptr(col),
              _ptr(val))
         return row, col, val, info
+
+    def level_spmv(self, level, which, x_ptr, y_ptr, nv, mode=0, stream=None):
+        """y = A x on the solver's own level matrix (device pointers)."""
+        call("XAMG_b200_solver_level_spmv", self.h, level, which, x_ptr, y_ptr, nv, mode,
+             stream if stream is not None else globals()["stream"]())
 
     def level_csr(self, level, which):
         d = Csr()

@@ -1,0 +1,92 @@
+"""The SpMV on a solver's own level matrices (XAMG_b200_solver_level_spmv),
+as its solves run it: the library's uploaded copy with XAMG's narrowing or
+2-byte relative columns, FP64 on the Krylov level and FP32 on the cycle's
+level 0 with gpu_precond_f32. Every element must equal the oracle's
+sequential row sum bit for bit, for y = A x and y += A x. The matrices mix
+banded rows with rows of far-off random columns, with row counts that leave
+ragged last tiles."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def banded_plus_random(n, far_from, n_far, seed):
+    """7-point band of a 3-D grid of n rows (plus-minus 1, nx, nx*ny), and
+    from row far_from on n_far extra random columns per row."""
+    rng = np.random.default_rng(seed)
+    nx, ny = 13, 11
+    row, cols, vals = [0], [], []
+    for i in range(n):
+        c = {i}
+        for o in (1, nx, nx * ny):
+            if i - o >= 0:
+                c.add(i - o)
+            if i + o < n:
+                c.add(i + o)
+        if i >= far_from:
+            c.update(int(v) for v in rng.integers(0, n, n_far))
+        c = sorted(c)
+        cols.extend(c)
+        vals.extend((rng.standard_normal(len(c)) + np.where(np.array(c) == i, 8.0, 0.0)).tolist())
+        row.append(len(cols))
+    return np.array(row, np.uint32), np.array(cols, np.uint32), np.array(vals, np.float64)
+
+
+def solver_on(gpu, row, col, val, nv, params):
+    M = gpu.Matrix(row, col, val)
+    xv, bv = gpu.Vector(M.n, nv), gpu.Vector(M.n, nv)
+    xv.set(0.0)
+    bv.set(1.0)
+    return M, xv, bv, gpu.Solver(M, gpu.Params(params), xv, bv)
+
+
+def run_level_spmv(gpu, S, level, which, row, col, val, nv, f32, seed):
+    import torch
+    n = len(row) - 1
+    dt = torch.float32 if f32 else torch.float64
+    rng = np.random.default_rng(seed)
+    xh = rng.uniform(-1, 1, n * nv).astype(np.float32 if f32 else np.float64)
+    y0 = rng.uniform(-1, 1, n * nv).astype(xh.dtype)
+    x = torch.from_numpy(xh).cuda()
+    y = torch.empty(n * nv, dtype=dt, device="cuda")
+    S.level_spmv(level, which, x.data_ptr(), y.data_ptr(), nv, 0)
+    ya = torch.from_numpy(y0).cuda()
+    S.level_spmv(level, which, x.data_ptr(), ya.data_ptr(), nv, 1)
+    torch.cuda.synchronize()
+    return xh, y0, y.cpu().numpy(), ya.cpu().numpy()
+
+
+KRYLOV = {"solver": {"method": "MergedPBiCGStab", "rel_tolerance": 1e-8, "max_iters": 10},
+          "preconditioner": {"method": "Jacobi"}}
+
+
+@pytest.mark.parametrize("nv", [2, 4, 8, 16, 32])
+@pytest.mark.parametrize("n,far_from", [(3001, 2400), (2000, 2000), (257, 200)])
+def test_fp64_level_spmv_bit_exact(gpu, oracle, nv, n, far_from):
+    row, col, val = banded_plus_random(n, far_from, 9, seed=n + nv)
+    _, _, _, S = solver_on(gpu, row, col, val, nv, KRYLOV)
+    xh, y0, y, ya = run_level_spmv(gpu, S, 0, 0, row, col, val, nv, False, seed=nv)
+    want = oracle.csr_ax_y(row, col, val, xh, nv)
+    assert y.tobytes() == want.tobytes()
+    want_a = oracle.csr_ax_y(row, col, val, xh, nv, axpy_y=y0)
+    assert ya.tobytes() == want_a.tobytes()
+
+
+@pytest.mark.parametrize("nv", [4, 8, 32])
+def test_fp32_cycle_operator_bit_exact(gpu, oracle, nv):
+    """Level 0 of an FP32 multigrid preconditioner (gpu_precond_f32 = 1),
+    with 2-byte relative columns, on a 27-point FE matrix."""
+    row, col, val = gpu.generate_diffusion(27, 14, 13, 12, 1.0, 1.0, 3)
+    params = {"solver": {"method": "MergedPBiCGStab", "rel_tolerance": 1e-8, "max_iters": 5,
+                         "gpu_index_compress": 2},
+              "preconditioner": {"method": "MultiGrid", "mg_max_levels": 3,
+                                 "gpu_precond_f32": 1, "gpu_index_compress": 2},
+              "pre_smoother": {"method": "Chebyshev"}, "post_smoother": {"method": "Chebyshev"}}
+    _, _, _, S = solver_on(gpu, row, col, val, nv, params)
+    info = S.level_info(0, 3)
+    assert info["f32"]
+    xh, y0, y, ya = run_level_spmv(gpu, S, 0, 3, row, col, val, nv, True, seed=nv)
+    v32 = val.astype(np.float32)
+    assert y.tobytes() == oracle.csr_ax_y(row, col, v32, xh, nv).tobytes()
+    assert ya.tobytes() == oracle.csr_ax_y(row, col, v32, xh, nv, axpy_y=y0).tobytes()
