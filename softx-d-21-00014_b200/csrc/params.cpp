@@ -316,7 +316,7 @@ SolverCfg resolve_cfg(const PList &l, const std::string &role) {
     c.gpu_coarse_f64 = l.get_i("gpu_coarse_f64", 0);
     c.gpu_index_compress = l.get_i("gpu_index_compress", 1);
     c.gpu_hsgs_rows = l.get_i("gpu_hsgs_rows", 32);
-    c.gpu_graph = l.get_i("gpu_graph", 0);
+    c.gpu_graph = l.get_i("gpu_graph", 1);
     c.gpu_seed = l.get_i("gpu_seed", 0);
     return c;
 }

@@ -78,7 +78,7 @@ struct SolverCfg {
     int gpu_coarse_f64 = 0;     // keep the Direct coarse solve in FP64 when reduced
     int gpu_index_compress = 1; // XAMG narrowing of column indices on upload
     int gpu_hsgs_rows = 32;     // target rows per hybrid Gauss-Seidel block
-    int gpu_graph = 0;          // capture the iteration as a CUDA graph
+    int gpu_graph = 1;          // replay preconditioner applications as CUDA graphs
     int gpu_seed = 0;           // seed of the host setup's random choices
 };
 

@@ -665,13 +665,67 @@ bool Krylov::check(const double *res, const double *res0, std::vector<double> &i
     return done;
 }
 
-void Krylov::apply_M(DVec &out, DVec &in) {
-    // set_const(out, 0) then precond->solve(out, in) with conv = ones
-    out.zero = true;
-    out.init = true;
+void Krylov::run_M(DVec &out, DVec &in) {
     static const std::vector<double> ones(32, 1.0);
     std::vector<double> o(ones.begin(), ones.begin() + NV);
     M->solve(out, in, o);
+}
+
+Krylov::~Krylov() {
+    for (auto &kv : graphs_)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+}
+
+// set_const(out, 0) then precond->solve(out, in) with conv = ones. With
+// gpu_graph (default) the application is recorded once per (out, in,
+// in.zero) as a CUDA graph, on its second call (the first one settles every
+// buffer and flag of the preconditioner), and replayed from then on: the
+// same kernels on the same buffers in one launch. A preconditioner whose
+// application cannot be captured runs directly.
+void Krylov::apply_M(DVec &out, DVec &in) {
+    out.zero = true;
+    out.init = true;
+    if (!cfg.gpu_graph) {
+        run_M(out, in);
+        return;
+    }
+    MGraph &g = graphs_[std::make_tuple(out.p<const void>(), in.p<const void>(), in.zero)];
+    if (g.exec) {
+        XG_CUDA(cudaGraphLaunch(g.exec, S()));
+        g_kernel_launches += g.launches;
+        out.zero = g.out_zero;
+        return;
+    }
+    if (g.failed || g.calls++ < 1) {
+        run_M(out, in);
+        return;
+    }
+    XG_CUDA(cudaStreamSynchronize(S()));
+    XG_CUDA(cudaStreamBeginCapture(S(), cudaStreamCaptureModeThreadLocal));
+    const uint64_t l0 = g_kernel_launches;
+    cudaGraph_t graph = nullptr;
+    bool ok = true;
+    try {
+        run_M(out, in);  // recorded, not run
+    } catch (...) {
+        ok = false;  // e.g. a preconditioner that reads back a residual
+    }
+    const cudaError_t e = cudaStreamEndCapture(S(), &graph);
+    if (!ok || e != cudaSuccess || !graph ||
+        cudaGraphInstantiate(&g.exec, graph, 0) != cudaSuccess) {
+        // nothing ran during the capture: run directly from now on
+        cudaGetLastError();
+        if (graph) cudaGraphDestroy(graph);
+        g.exec = nullptr;
+        g.failed = true;
+        g_kernel_launches = l0;
+        run_M(out, in);
+        return;
+    }
+    cudaGraphDestroy(graph);
+    g.launches = g_kernel_launches - l0;
+    g.out_zero = out.zero;
+    XG_CUDA(cudaGraphLaunch(g.exec, S()));
 }
 
 void Krylov::solve(DVec &x, DVec &b, const std::vector<double> &conv) {

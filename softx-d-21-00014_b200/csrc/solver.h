@@ -6,6 +6,7 @@
 #pragma once
 
 #include <map>
+#include <tuple>
 #include <memory>
 #include <string>
 #include <vector>
@@ -75,6 +76,17 @@ class MultiGrid : public SolverBase {
     void cycle(int level, DVec &x, DVec &b, int cyc, const std::vector<double> &iconv);
 };
 
+// A preconditioner application captured as a CUDA graph: the kernels that
+// M->solve(out, in) launches for one (out, in, in.zero) combination, and the
+// zero flag it leaves on out.
+struct MGraph {
+    cudaGraphExec_t exec = nullptr;
+    int calls = 0;          // direct runs before the capture
+    bool failed = false;    // capture not possible: always run directly
+    bool out_zero = false;
+    uint64_t launches = 0;  // kernels in the graph
+};
+
 class Krylov : public SolverBase {
   public:
     bool precond_form = true;  // (P)BiCGStab structure; false: MergedBiCGStab
@@ -82,11 +94,14 @@ class Krylov : public SolverBase {
     DevBuf sc;                 // scalar block (kernels.cuh Sc)
     void setup() override;
     void solve(DVec &x, DVec &b, const std::vector<double> &conv) override;
+    ~Krylov() override;
 
   private:
     bool check(const double *res, const double *res0, std::vector<double> &iconv);
     void apply_M(DVec &out, DVec &in);
+    void run_M(DVec &out, DVec &in);
     void upload_iconv(const std::vector<double> &iconv);
+    std::map<std::tuple<const void *, const void *, bool>, MGraph> graphs_;
 };
 
 // The solver hierarchy of XAMG_solver_create* (construct_solver_hierarchy,
