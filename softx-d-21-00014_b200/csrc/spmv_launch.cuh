@@ -67,13 +67,31 @@ static uint32_t tile_max(const DCsr &A, int nv, cudaStream_t s) {
 }
 
 // Staging buffers: one buffer holds cap entries of values and columns (plus
-// alignment slack); two buffers (the copy of the next tile overlapping the
-// current one) while they fit in 48 KB, at least four blocks per SM; else one
-// buffer of up to 96 KB.
+// alignment slack). Two buffers let the copy of a block's next tile overlap
+// its current one, one buffer lets more blocks share an SM: the launcher
+// takes two unless that lowers the number of resident blocks (measured on the
+// 27-point 128^3 matrix: nv = 4 runs 10 % faster on one buffer and twice the
+// blocks, nv = 8 and 16 about 10 % faster on two at equal blocks). Buffers
+// hold at most 96 KB.
 template <typename F, typename I>
 static uint32_t stage_buffer_bytes(uint32_t cap) {
     auto r16 = [](uint64_t b) { return (uint32_t)((b + 15) & ~(uint64_t)15); };
     return r16((uint64_t)cap * sizeof(F) + 32) + r16((uint64_t)cap * sizeof(I) + 32);
+}
+
+// Resident blocks per SM of a kernel for a dynamic shared-memory size
+// (remembered per kernel and size).
+template <class Kern>
+static int resident_blocks(Kern kern, int threads, size_t smem) {
+    static std::map<std::pair<const void *, size_t>, int> cache;
+    const auto key = std::make_pair((const void *)kern, smem);
+    auto it = cache.find(key);
+    if (it == cache.end()) {
+        int nb = 0;
+        XG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, threads, smem));
+        it = cache.emplace(key, std::max(nb, 1)).first;
+    }
+    return it->second;
 }
 
 // Grid: as many blocks as fit the GPU at once (one wave). With dot products
@@ -82,6 +100,7 @@ static uint32_t stage_buffer_bytes(uint32_t cap) {
 template <typename F, typename FX, typename I, int NV, int VK, int NRED, class Epi>
 static void launch_vk(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s) {
     constexpr uint32_t LIMIT1 = (96u * 1024u - 64u) / (uint32_t)(sizeof(F) + sizeof(I));
+    constexpr int NT = k::CT / VK;
     auto kern = k::k_spmv<F, FX, I, NV, VK, NRED, Epi>;
     static bool big_smem = false;  // one flag per instantiation
     if (!big_smem) {
@@ -89,27 +108,26 @@ static void launch_vk(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s
                                      (int)stage_buffer_bytes<F, I>(LIMIT1)));
         big_smem = true;
     }
-    const uint32_t tm = tile_max(A, NV, s);
-    uint32_t cap = tm, nbuf = 2;
-    if (2 * stage_buffer_bytes<F, I>(tm) > 48u * 1024u) {
-        nbuf = 1;
-        cap = std::min(tm, LIMIT1);
+    const uint32_t cap = std::min(tile_max(A, NV, s), LIMIT1);
+    const size_t one = stage_buffer_bytes<F, I>(cap);
+    const int res1 = resident_blocks(kern, NT, one);
+    uint32_t nbuf = 1;
+    int res = res1;
+    if (2 * one <= (size_t)stage_buffer_bytes<F, I>(LIMIT1)) {
+        const int res2 = resident_blocks(kern, NT, 2 * one);
+        if (res2 >= res1) {
+            nbuf = 2;
+            res = res2;
+        }
     }
-    const size_t smem = (size_t)nbuf * stage_buffer_bytes<F, I>(cap);
-    static std::map<size_t, int> resident;  // per instantiation: blocks per SM by smem
-    auto it = resident.find(smem);
-    if (it == resident.end()) {
-        int nb = 0;
-        XG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, k::CT / VK, smem));
-        it = resident.emplace(smem, std::max(nb, 1)).first;
-    }
+    const size_t smem = nbuf * one;
     const uint64_t R = k::CT / NV;
     const uint64_t ntiles = (A.nrows + R - 1) / R;
-    const uint64_t wave = (uint64_t)it->second * (uint64_t)ctx().sms;
+    const uint64_t wave = (uint64_t)res * (uint64_t)ctx().sms;
     const uint32_t B = NRED > 0 ? (uint32_t)k::canon_blocks(A.nrows, NV)
                                 : (uint32_t)std::min<uint64_t>(ntiles, wave);
     const uint32_t P = (uint32_t)std::min<uint64_t>(B, wave);
-    kern<<<P, k::CT / VK, smem, s>>>(A.args<F>(), x, epi, ctx().red(), cap, nbuf, B);
+    kern<<<P, NT, smem, s>>>(A.args<F>(), x, epi, ctx().red(), cap, nbuf, B);
     XG_CUDA(cudaGetLastError());
     ++g_kernel_launches;
 }
