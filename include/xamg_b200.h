@@ -148,6 +148,33 @@ int XAMG_b200_solver_hierarchy_export(size_t sid, int level, int which, uint32_t
  * running the kernel entry points on the solver's own data (no counterpart). */
 int XAMG_b200_solver_level_csr(size_t sid, int level, int which, XAMG_b200_csr *out);
 
+/* XAMG's binary system file (src/io/detail/reader.inl:47-177, read by
+ * XAMG::io::read_system): u32 nrows, u32 nnz, u32 row[nrows+1], u32
+ * col[nnz], f64 val[nnz], then optionally f64 b[nrows*nv] and f64
+ * x[nrows*nv] ([row][rhs] interleaved). read_system_size gives the sizes to
+ * allocate; read_system fills row/col/val and, when not NULL, b and x, with
+ * b = 1 and x = 0 where the file holds none (as read_system does); *found
+ * gets bit 0 for b read, bit 1 for x read. write_system writes the same
+ * format (x only after b). The reference reads x from the start of the file
+ * (reader.inl:160, SEEK_SET with a relative offset); here x is read where it
+ * is stored, after b. */
+int XAMG_b200_read_system_size(const char *path, uint32_t *nrows, uint32_t *nnz);
+int XAMG_b200_read_system(const char *path, uint16_t nv, uint32_t *row, uint32_t *col,
+                          double *val, double *b, double *x, int *found);
+int XAMG_b200_write_system(const char *path, uint32_t nrows, uint32_t nnz, const uint32_t *row,
+                           const uint32_t *col, const double *val, uint16_t nv, const double *b,
+                           const double *x);
+
+/* Multigrid hierarchy files (no counterpart: the reference rebuilds the
+ * hierarchy through hypre on every run). save writes the host hierarchy a
+ * solver's multigrid was built from (every level but the finest, which is the
+ * matrix itself, the interpolations, the eigenvalue estimates) with its setup
+ * parameters and a fingerprint of the matrix; load attaches such a file to a
+ * constructed matrix with the same arrays, so that a solver created on it with
+ * the same multigrid setup parameters skips the setup. */
+int XAMG_b200_solver_hierarchy_save(size_t sid, const char *path);
+int XAMG_b200_matrix_hierarchy_load(size_t mid, const char *path);
+
 /* y = A x (mode 0) or y += A x (mode 1) with level matrix `which` of a
  * solver, as its solves run it: on the library's own copy, with the x-staging
  * plan it has for nv (no counterpart; the kernel-level view of the solver's

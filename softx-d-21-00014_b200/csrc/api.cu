@@ -14,6 +14,7 @@
 
 #include "../../include/xamg_c_api.h"
 #include "ops.h"
+#include "io.h"
 #include "solver.h"
 
 #ifndef XAMG_NV
@@ -857,6 +858,52 @@ int XAMG_b200_solver_level_csr(size_t sid, int level, int which, XAMG_b200_csr *
         out->val = d.val.p;
         out->col_bytes = d.col_bytes;
         out->val_f32 = d.f32;
+    });
+}
+
+int XAMG_b200_read_system_size(const char *path, uint32_t *nrows, uint32_t *nnz) {
+    return guarded([&] {
+        XG_REQUIRE(nrows && nnz, XAMG_ERR_INVALID_ARG, "null argument");
+        const SystemSize z = read_system_size(path);
+        *nrows = z.nrows;
+        *nnz = z.nnz;
+    });
+}
+
+int XAMG_b200_read_system(const char *path, uint16_t nv, uint32_t *row, uint32_t *col,
+                          double *val, double *b, double *x, int *found) {
+    return guarded([&] {
+        check_nv(nv);
+        const int f = read_system(path, nv, row, col, val, b, x);
+        if (found) *found = f;
+    });
+}
+
+int XAMG_b200_write_system(const char *path, uint32_t nrows, uint32_t nnz, const uint32_t *row,
+                           const uint32_t *col, const double *val, uint16_t nv, const double *b,
+                           const double *x) {
+    return guarded([&] {
+        check_nv(nv);
+        write_system(path, nrows, nnz, row, col, val, nv, b, x);
+    });
+}
+
+int XAMG_b200_solver_hierarchy_save(size_t sid, const char *path) {
+    return guarded([&] {
+        SolverObj &so = get(g_solvers, sid, "solver");
+        MultiGrid *mg = so.sh->mg;
+        XG_REQUIRE(mg && mg->H, XAMG_ERR_INVALID_ARG, "the solver has no multigrid hierarchy");
+        save_hierarchy(path, hierarchy_key(mg->cfg), so.sh->hA, *mg->H);
+    });
+}
+
+int XAMG_b200_matrix_hierarchy_load(XAMG_matrix_id mid, const char *path) {
+    return guarded([&] {
+        MatObj &m = get(g_mats, mid, "matrix");
+        XG_REQUIRE(m.constructed, XAMG_ERR_INVALID_ARG, "matrix not constructed");
+        std::string key;
+        auto H = load_hierarchy(path, m.h, key);
+        m.hcache[key] = H;
     });
 }
 

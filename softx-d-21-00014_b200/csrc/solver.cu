@@ -442,7 +442,7 @@ std::unique_ptr<SolverBase> make_smoother(const SolverCfg &cfg, const std::strin
 // ===========================================================================
 // MultiGrid (mg.inl:97-334)
 // ===========================================================================
-static std::string hierarchy_key(const SolverCfg &c) {
+std::string hierarchy_key(const SolverCfg &c) {
     char buf[256];
     snprintf(buf, sizeof(buf), "th=%.9g mrs=%.9g tf=%.9g pmax=%d ml=%d cs=%d ct=%d it=%d seed=%d",
              (double)c.mg_strength_threshold, (double)c.mg_max_row_sum, (double)c.mg_trunc_factor,

@@ -57,6 +57,8 @@ std::unique_ptr<SolverBase> make_smoother(const SolverCfg &cfg, const std::strin
 // they depend on (the reference rebuilds the hierarchy for every solver; here
 // solvers that differ only in precision or smoothers share one build).
 using HierCache = std::map<std::string, std::shared_ptr<const Hierarchy>>;
+// The cache key of a hierarchy: the setup parameters it was built with.
+std::string hierarchy_key(const SolverCfg &c);
 
 class MultiGrid : public SolverBase {
   public:

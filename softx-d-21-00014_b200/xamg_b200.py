@@ -55,7 +55,9 @@ EXT_SYMBOLS = [
     "XAMG_b200_solver_hierarchy_export", "XAMG_b200_vector_device_ptr",
     "XAMG_b200_solver_level_csr", "XAMG_b200_kernel_launches", "XAMG_b200_stream",
     "XAMG_b200_set_device", "XAMG_b200_dot_noalloc", "XAMG_b200_wait_selftest",
-    "XAMG_b200_solver_level_spmv",
+    "XAMG_b200_solver_level_spmv", "XAMG_b200_read_system_size", "XAMG_b200_read_system",
+    "XAMG_b200_write_system", "XAMG_b200_solver_hierarchy_save",
+    "XAMG_b200_matrix_hierarchy_load",
 ]
 
 
@@ -172,6 +174,14 @@ def lib():
         "XAMG_b200_wait_selftest": (C.c_int, [C.c_double, C.POINTER(C.c_int)]),
         "XAMG_b200_solver_level_spmv": (C.c_int, [C.c_size_t, C.c_int, C.c_int, vp, vp, C.c_int,
                                                   C.c_int, vp]),
+        "XAMG_b200_read_system_size": (C.c_int, [C.c_char_p, C.POINTER(C.c_uint32),
+                                                 C.POINTER(C.c_uint32)]),
+        "XAMG_b200_read_system": (C.c_int, [C.c_char_p, C.c_uint16, vp, vp, vp, vp, vp,
+                                            C.POINTER(C.c_int)]),
+        "XAMG_b200_write_system": (C.c_int, [C.c_char_p, C.c_uint32, C.c_uint32, vp, vp, vp,
+                                             C.c_uint16, vp, vp]),
+        "XAMG_b200_solver_hierarchy_save": (C.c_int, [C.c_size_t, C.c_char_p]),
+        "XAMG_b200_matrix_hierarchy_load": (C.c_int, [C.c_size_t, C.c_char_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -205,6 +215,34 @@ def _ptr(a):
 
 
 # ---------------------------------------------------------------- generators
+def read_system(path, nv=1):
+    """XAMG's binary system file: (row, col, val, b, x, found) with b, x as
+    [n*nv] arrays (b = 1, x = 0 where the file holds none; found bit 0/1)."""
+    n, nnz = C.c_uint32(), C.c_uint32()
+    call("XAMG_b200_read_system_size", str(path).encode(), C.byref(n), C.byref(nnz))
+    row = np.zeros(n.value + 1, np.uint32)
+    col = np.zeros(nnz.value, np.uint32)
+    val = np.zeros(nnz.value, np.float64)
+    b = np.zeros(n.value * nv, np.float64)
+    x = np.zeros(n.value * nv, np.float64)
+    found = C.c_int()
+    call("XAMG_b200_read_system", str(path).encode(), nv, _ptr(row), _ptr(col), _ptr(val),
+         _ptr(b), _ptr(x), C.byref(found))
+    return row, col, val, b, x, found.value
+
+
+def write_system(path, row, col, val, nv=1, b=None, x=None):
+    """Write XAMG's binary system file (x only together with b)."""
+    row = np.ascontiguousarray(row, np.uint32)
+    col = np.ascontiguousarray(col, np.uint32)
+    val = np.ascontiguousarray(val, np.float64)
+    bb = None if b is None else np.ascontiguousarray(b, np.float64)
+    xx = None if x is None else np.ascontiguousarray(x, np.float64)
+    call("XAMG_b200_write_system", str(path).encode(), len(row) - 1, len(col), _ptr(row),
+         _ptr(col), _ptr(val), nv, None if bb is None else _ptr(bb),
+         None if xx is None else _ptr(xx))
+
+
 def generate_cube(nx, ny, nz):
     """The reference's 7-point Laplacian (cube.inl) as numpy CSR arrays."""
     n = nx * ny * nz
@@ -315,6 +353,11 @@ class Matrix:
         call("XAMG_csr_matrix_destroy", c.value)
         self.h, self.part, self.n, self.nnz = m.value, p.value, n, len(col)
 
+    def load_hierarchy(self, path):
+        """Attach a hierarchy file written for this matrix (skips the setup of
+        solvers created with the same multigrid parameters)."""
+        call("XAMG_b200_matrix_hierarchy_load", self.h, str(path).encode())
+
 
 class Vector:
     """XAMG_vector_* of n rows and nv interleaved right-hand sides (device)."""
@@ -398,6 +441,10 @@ class Solver:
         call("XAMG_b200_solver_level_download", self.h, level, which, _ptr(row), _ptr(col),
              _ptr(val))
         return row, col, val, info
+
+    def save_hierarchy(self, path):
+        """Write the multigrid hierarchy this solver was built from."""
+        call("XAMG_b200_solver_hierarchy_save", self.h, str(path).encode())
 
     def level_spmv(self, level, which, x_ptr, y_ptr, nv, mode=0, stream=None):
         """y = A x on the solver's own level matrix (device pointers)."""
