@@ -1717,6 +1717,45 @@ static void solve_bicgstab(Solver &S, Vec &x, Vec &b, const Vec &conv, bool prec
     } while (it < S.sp.max_iters);
 }
 
+// pcg.inl:44-162: preconditioned conjugate gradients (the preconditioner is
+// the identity when no preconditioner list is given)
+static void solve_pcg(Solver &S, Vec &x, Vec &b, const Vec &conv) {
+    typedef double F;
+    const int NV = S.NV;
+    reset_stats(S);
+    int &it = S.st.iters;
+    Vec iconv = conv;
+    Vec a1 = typed_scalar<F>(NV, 1.0), a_1 = typed_scalar<F>(NV, -1.0);
+    Vec rho0 = make_vec<F>(1, NV), res = make_vec<F>(1, NV);
+    Vec scal1 = make_vec<F>(1, NV), scal2 = make_vec<F>(1, NV), scal3 = make_vec<F>(1, NV);
+    Vec alpha = make_vec<F>(1, NV), beta = make_vec<F>(1, NV), alpha_conv = make_vec<F>(1, NV);
+    for (auto &v : S.buf) blas::set_const<F>(v, 0.0);
+    Vec &r = S.buf[0], &z = S.buf[1], &p = S.buf[2], &Ap = S.buf[3];
+    get_residual<F>(S, x, b, r, rho0, S.sp.convergence_check != 0);
+    if (converged<F>(S, rho0, rho0, iconv)) return;
+    blas::set_const<F>(z, 0.0);
+    precond_apply(S, z, r);
+    blas::copy<F>(z, p);
+    do {
+        ++it;
+        blas2::Ax_y<F>(*S.A, p, Ap);
+        blas::dot<F>(r, z, scal1);
+        blas::dot<F>(p, Ap, scal2);
+        blas::xdivy_z<F>(scal1, scal2, alpha);
+        blas::ax_y<F>(iconv, alpha, alpha_conv);
+        blas::axpby<F>(alpha_conv, p, a1, x);
+        blas::scal<F>(a_1, alpha);
+        blas::axpby<F>(alpha, Ap, a1, r);
+        blas::set_const<F>(z, 0.0);
+        precond_apply(S, z, r);
+        blas::dot<F>(r, z, scal3);
+        blas::xdivy_z<F>(scal3, scal1, beta);
+        blas::axpby<F>(a1, z, beta, p);
+        blas::dot<F>(r, r, res);
+        if (converged<F>(S, res, rho0, iconv)) return;
+    } while (it < S.sp.max_iters);
+}
+
 template <typename T>
 static void solve(Solver &S, Vec &x, Vec &b, const Vec &conv) {
     const std::string &m = S.method;
@@ -1740,6 +1779,8 @@ static void solve(Solver &S, Vec &x, Vec &b, const Vec &conv) {
         solve_bicgstab(S, x, b, conv, false);
     else if (m == "PBiCGStab")
         solve_bicgstab(S, x, b, conv, true);
+    else if (m == "PCG")
+        solve_pcg(S, x, b, conv);
 }
 
 // ----------------------------------------------------------------------------
@@ -1761,6 +1802,7 @@ static int buffer_nvecs(const std::string &m) {
     if (m == "Chebyshev") return 3;
     if (m == "MultiGrid") return 1;
     if (m == "BiCGStab") return 6;
+    if (m == "PCG") return 4;
     if (m == "PBiCGStab" || m == "MergedBiCGStab" || m == "MergedPBiCGStab") return 8;
     return 0;
 }

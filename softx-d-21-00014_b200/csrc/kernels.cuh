@@ -865,6 +865,86 @@ struct OpXUpdate {
     }
 };
 
+// PCG (pcg.inl:103-150). Ap = A p with scal2 = (p, Ap); finaliser:
+// alpha = scal1 / scal2, alpha_conv = iconv * alpha, then alpha = -1 * alpha
+// (kept in SC_NSCAL). scal1 = (r, z) is the previous (r, z) (EPcgDots).
+template <int NV>
+struct EPcgAp {
+    double *Ap;
+    const double *p;
+    double *sc;
+    __device__ double init(uint64_t, int) const { return 0.0; }
+    template <int NR>
+    __device__ void store(uint64_t i, int k, double y, double (&acc)[NR]) const {
+        const uint64_t e = i * NV + k;
+        Ap[e] = y;
+        acc[0] = add(acc[0], mul(p[e], y));
+    }
+    __device__ void operator()(int k, const double *s) const {
+        double *S = sc;
+        S[SC_SCAL2 * SC_STRIDE + k] = s[0];
+        const double alpha = dvd(S[SC_SCAL1 * SC_STRIDE + k], s[0]);
+        S[SC_ALPHA * SC_STRIDE + k] = alpha;
+        S[SC_ALPHA_C * SC_STRIDE + k] = mul(S[SC_ICONV * SC_STRIDE + k], alpha);
+        S[SC_NSCAL * SC_STRIDE + k] = mul(-1.0, alpha);
+    }
+};
+
+// (r, z) and (r, r) in one pass; finaliser: first call scal1 = (r, z);
+// afterwards scal3 = (r, z), beta = scal3 / scal1, res = (r, r), and
+// scal1 = scal3 for the next iteration (XAMG recomputes dot(r, z) there from
+// the same vectors, pcg.inl:105).
+template <int NV>
+struct EPcgDots {
+    const double *r, *z;
+    double *sc;
+    bool first;
+    template <int NR>
+    __device__ void elem(uint64_t i, int k, double (&acc)[NR]) const {
+        const uint64_t e = i * NV + k;
+        const double rv = r[e];
+        acc[0] = add(acc[0], mul(rv, z[e]));
+        acc[1] = add(acc[1], mul(rv, rv));
+    }
+    __device__ void operator()(int k, const double *s) const {
+        double *S = sc;
+        if (first) {
+            S[SC_SCAL1 * SC_STRIDE + k] = s[0];
+            return;
+        }
+        S[SC_SCAL3 * SC_STRIDE + k] = s[0];
+        S[SC_BETA * SC_STRIDE + k] = dvd(s[0], S[SC_SCAL1 * SC_STRIDE + k]);
+        S[SC_SCAL1 * SC_STRIDE + k] = s[0];
+        S[SC_RES * SC_STRIDE + k] = s[1];
+    }
+};
+
+// x = alpha_conv*p + 1*x (x = alpha_conv*p while x is zero-flagged);
+// r = (-alpha)*Ap + 1*r  (pcg.inl:123-127, axpby blas.inl:89-151)
+struct OpPcgXR {
+    double *x, *r;
+    const double *p, *Ap, *sc;
+    int nv;
+    bool x_zero;
+    __device__ void operator()(uint64_t e) const {
+        const int k = (int)(e % nv);
+        const double ac = sc[SC_ALPHA_C * SC_STRIDE + k], na = sc[SC_NSCAL * SC_STRIDE + k];
+        x[e] = x_zero ? mul(ac, p[e]) : add(mul(ac, p[e]), mul(1.0, x[e]));
+        r[e] = add(mul(na, Ap[e]), mul(1.0, r[e]));
+    }
+};
+
+// p = 1*z + beta*p  (pcg.inl:142)
+struct OpPcgP {
+    double *p;
+    const double *z, *sc;
+    int nv;
+    __device__ void operator()(uint64_t e) const {
+        const int k = (int)(e % nv);
+        p[e] = add(mul(1.0, z[e]), mul(sc[SC_BETA * SC_STRIDE + k], p[e]));
+    }
+};
+
 // p = 1*r + nscal*v + beta*p  (merged_pbicgstab.inl:216-218)
 struct OpPUpdate {
     double *p;

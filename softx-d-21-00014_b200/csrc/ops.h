@@ -37,6 +37,14 @@ void spmv_dot_alpha(const DCsr &A, const double *pa, double *v, const double *r0
                     int nv, cudaStream_t s);
 
 // t = A sa; phi, psi, theta; omega; res; alpha_c; omega_c
+// PCG: Ap = A p with (p, Ap) and alpha; (r, z) and (r, r) with beta;
+// x, r updates; p = z + beta p (pcg.inl:103-150)
+void pcg_ap(const DCsr &A, const double *p, double *Ap, double *sc, int nv, cudaStream_t s);
+void pcg_dots(uint64_t n, const double *r, const double *z, double *sc, bool first, int nv,
+              cudaStream_t s);
+void pcg_xr(uint64_t n, double *x, double *r, const double *p, const double *Ap,
+            const double *sc, bool x_zero, int nv, cudaStream_t s);
+void pcg_p(uint64_t n, double *p, const double *z, const double *sc, int nv, cudaStream_t s);
 void spmv_dot3(const DCsr &A, const double *sa, double *t, const double *s_, double *sc, int nv,
                cudaStream_t s);
 

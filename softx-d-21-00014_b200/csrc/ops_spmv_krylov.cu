@@ -49,6 +49,18 @@ void spmv_dot_alpha(const DCsr &A, const double *pa, double *v, const double *r0
     });
 }
 
+void pcg_ap(const DCsr &A, const double *p, double *Ap, double *sc, int nv, cudaStream_t s) {
+    XG_DISPATCH(A, nv, { launch<double, double, I, NV, 1>(A, p, k::EPcgAp<NV>{Ap, p, sc}, s); });
+}
+
+void pcg_dots(uint64_t n, const double *r, const double *z, double *sc, bool first, int nv,
+              cudaStream_t s) {
+    dispatch_nv(nv, [&](auto nvc) {
+        constexpr int NV = decltype(nvc)::value;
+        launch_rows<double, NV, 2>(n, k::EPcgDots<NV>{r, z, sc, first}, s);
+    });
+}
+
 void spmv_dot3(const DCsr &A, const double *sa, double *t, const double *s_, double *sc, int nv,
                cudaStream_t s) {
     XG_DISPATCH(A, nv, { launch<double, double, I, NV, 3>(A, sa, k::EDot3<NV>{t, s_, sc}, s); });

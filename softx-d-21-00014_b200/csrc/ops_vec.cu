@@ -86,6 +86,13 @@ void p_update(uint64_t n, double *p, const double *r, const double *v, const dou
               cudaStream_t s) {
     flat(n * nv, k::OpPUpdate{p, r, v, sc, nv}, s);
 }
+void pcg_xr(uint64_t n, double *x, double *r, const double *p, const double *Ap,
+            const double *sc, bool x_zero, int nv, cudaStream_t s) {
+    flat(n * nv, k::OpPcgXR{x, r, p, Ap, sc, nv, x_zero}, s);
+}
+void pcg_p(uint64_t n, double *p, const double *z, const double *sc, int nv, cudaStream_t s) {
+    flat(n * nv, k::OpPcgP{p, z, sc, nv}, s);
+}
 void group5(uint64_t n, double *x, double *p, const double *s_, const double *r, const double *v,
             const double *sc, int nv, cudaStream_t s) {
     flat(n * nv, k::OpGroup5{x, p, s_, r, v, sc, nv}, s);

@@ -728,8 +728,50 @@ void Krylov::apply_M(DVec &out, DVec &in) {
     XG_CUDA(cudaGraphLaunch(g.exec, S()));
 }
 
+// pcg.inl:44-162: fused as Ap = A p with (p, Ap) and alpha; the x and r
+// updates; z = M^-1 r; (r, z), (r, r) and beta; p = z + beta p. The first
+// (r, z) comes from the same dot kernel after z0 = M^-1 r0.
+void Krylov::solve_pcg(DVec &x, DVec &b, const std::vector<double> &conv) {
+    cudaStream_t s = S();
+    std::vector<double> iconv = conv;
+    upload_iconv(iconv);
+    double *SC = sc.as<double>();
+    for (auto &v : buf) {
+        v.zero = true;
+        v.init = true;
+    }
+    DVec &r = buf[0], &z = buf[1], &p = buf[2], &Ap = buf[3];
+    std::vector<double> rho0(NV), res(NV);
+    residual_norm<double>(*A, x, b, r, NV, rho0.data());
+    if (check(rho0.data(), rho0.data(), iconv)) return;
+    apply_M(z, r);
+    // copy(z, p), zero flag included (blas.inl:224-246)
+    p.zero = z.zero;
+    if (!z.zero) ops::convert<double, double>(p.p<double>(), z.p<double>(), p.elems(), s);
+    ops::pcg_dots(n, r.p<double>(), z.p<double>(), SC, true, NV, s);
+    do {
+        ++st.iters;
+        ops::pcg_ap(*A, p.p<double>(), Ap.p<double>(), SC, NV, s);
+        Ap.zero = false;
+        ops::pcg_xr(n, x.p<double>(), r.p<double>(), p.p<double>(), Ap.p<double>(), SC, x.zero,
+                    NV, s);
+        x.zero = false;
+        x.init = true;
+        apply_M(z, r);
+        ops::pcg_dots(n, r.p<double>(), z.p<double>(), SC, false, NV, s);
+        ops::pcg_p(n, p.p<double>(), z.p<double>(), SC, NV, s);
+        read_scalars(SC + k::SC_RES * k::SC_STRIDE, res.data(), NV);
+        if (check(res.data(), rho0.data(), iconv)) return;
+    } while (st.iters < cfg.max_iters);
+    XG_CUDA(cudaStreamSynchronize(s));
+}
+
 void Krylov::solve(DVec &x, DVec &b, const std::vector<double> &conv) {
     reset_stats();
+    if (pcg) {
+        solve_pcg(x, b, conv);
+        return;
+    }
     cudaStream_t s = S();
     std::vector<double> iconv = conv;
     upload_iconv(iconv);
@@ -820,7 +862,8 @@ void SolverHierarchy::build(const Params &P, const HCsr &hA_, const DCsr *A_, in
         root.reset(g);
         return;
     }
-    if (m == "MergedPBiCGStab" || m == "PBiCGStab" || m == "MergedBiCGStab" || m == "BiCGStab") {
+    if (m == "MergedPBiCGStab" || m == "PBiCGStab" || m == "MergedBiCGStab" || m == "BiCGStab" ||
+        m == "PCG") {
         auto *kr = new Krylov();
         kr->cfg = c;
         kr->role = "solver";
@@ -828,8 +871,9 @@ void SolverHierarchy::build(const Params &P, const HCsr &hA_, const DCsr *A_, in
         kr->A = A;
         kr->n = hA.nrows;
         kr->precond_form = (m != "MergedBiCGStab");
+        kr->pcg = (m == "PCG");
         kr->setup();
-        const bool wants_M = (m == "MergedPBiCGStab" || m == "PBiCGStab");
+        const bool wants_M = (m == "MergedPBiCGStab" || m == "PBiCGStab" || m == "PCG");
         if (wants_M && P.has("preconditioner")) {
             SolverCfg pc = resolve_cfg(P.get("preconditioner"), "preconditioner");
             if (pc.method == "MultiGrid") {

@@ -92,6 +92,7 @@ struct MGraph {
 class Krylov : public SolverBase {
   public:
     bool precond_form = true;  // (P)BiCGStab structure; false: MergedBiCGStab
+    bool pcg = false;          // preconditioned conjugate gradients (pcg.inl)
     std::unique_ptr<SolverBase> M;
     DevBuf sc;                 // scalar block (kernels.cuh Sc)
     void setup() override;
@@ -102,6 +103,7 @@ class Krylov : public SolverBase {
     bool check(const double *res, const double *res0, std::vector<double> &iconv);
     void apply_M(DVec &out, DVec &in);
     void run_M(DVec &out, DVec &in);
+    void solve_pcg(DVec &x, DVec &b, const std::vector<double> &conv);
     void upload_iconv(const std::vector<double> &iconv);
     std::map<std::tuple<const void *, const void *, bool>, MGraph> graphs_;
 };

@@ -93,15 +93,32 @@ def test_config1_merged_pbicgstab_jacobi(gpu, oracle):
     assert S.level_info(0, 0)["col_bytes"] == 2
 
 
-@pytest.mark.parametrize("method", ["PBiCGStab", "BiCGStab", "MergedBiCGStab"])
+@pytest.mark.parametrize("method", ["PBiCGStab", "BiCGStab", "MergedBiCGStab", "PCG"])
 @pytest.mark.parametrize("nv", [2, 8])
 def test_krylov_variants(gpu, oracle, method, nv):
     row, col, val = gpu.generate_cube(14, 13, 12)
     params = {"solver": {"method": method, "max_iters": 500, "rel_tolerance": 1e-9,
                          "abs_tolerance": 0}}
-    if method == "PBiCGStab":
+    if method in ("PBiCGStab", "PCG"):
         params["preconditioner"] = {"method": "Jacobi", "max_iters": 3}
     check(gpu, oracle, row, col, val, nv, params, seed=nv, tol=1e-9)
+
+
+@pytest.mark.parametrize("precond", [None, "MultiGrid"])
+def test_pcg(gpu, oracle, precond):
+    """PCG (pcg.inl:44-162): unpreconditioned (the identity) and with an AMG
+    V-cycle (Jacobi smoothing keeps the preconditioner symmetric)."""
+    row, col, val = gpu.generate_diffusion(7, 15, 14, 13, 1.0, 1.0, 6)
+    nv = 4
+    params = {"solver": {"method": "PCG", "max_iters": 400, "rel_tolerance": 1e-8,
+                         "abs_tolerance": 0}}
+    if precond:
+        params["preconditioner"] = dict(MG_BASE, method="MultiGrid")
+        params["pre_smoother"] = {"method": "Jacobi"}
+        params["post_smoother"] = {"method": "Jacobi"}
+        params["coarse_grid_solver"] = {"method": "Direct"}
+    st, S = check(gpu, oracle, row, col, val, nv, params, seed=3)
+    assert st["iters"] < (40 if precond else 400)
 
 
 @pytest.mark.parametrize("smoother,reduced", [("Jacobi", 0), ("Chebyshev", 0), ("HSGS", 0),
