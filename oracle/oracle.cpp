@@ -644,6 +644,67 @@ void merged_bicgstab_group5(Vec &x, Vec &p, Vec &s, Vec &r, Vec &v, const Vec &a
 }
 
 // blas_merged_jacobi.inl:32-90
+// blas_merged_rbicgstab.inl:33-116: r = r - alpha v; theta = (t, r),
+// phi = (t, t), psi = (t, r0), eta = (r, r)
+template <typename T>
+void merged_rbicgstab_group1(Vec &r, Vec &v, Vec &t, Vec &r0, const Vec &alpha, Vec &theta,
+                             Vec &phi, Vec &psi, Vec &eta) {
+    if (r.zero) set_const<T>(r, 0.0, true);
+    if (v.zero) forced_set_const<T>(v, 0.0);
+    if (t.zero) forced_set_const<T>(t, 0.0);
+    if (r0.zero) forced_set_const<T>(r0, 0.0);
+    const int NV = r.nv;
+    T *rp = r.p<T>();
+    const T *vp = v.p<T>(), *tp = t.p<T>(), *r0p = r0.p<T>(), *ap = alpha.p<T>();
+    for (uint64_t i = 0; i < NV * r.size; i += NV)
+        for (int k = 0; k < NV; ++k) rp[i + k] = rp[i + k] - ap[k] * vp[i + k];
+    std::vector<T> out(4 * NV);
+    reduce<T>(r.size, NV, 4,
+              [&](uint64_t i, int k, T *o) {
+                  const T tv = tp[i * NV + k], rv = rp[i * NV + k];
+                  o[0] = tv * rv;
+                  o[1] = tv * tv;
+                  o[2] = tv * r0p[i * NV + k];
+                  o[3] = rv * rv;
+              },
+              out.data());
+    for (int k = 0; k < NV; ++k) {
+        theta.p<T>()[k] = out[k * 4 + 0];
+        phi.p<T>()[k] = out[k * 4 + 1];
+        psi.p<T>()[k] = out[k * 4 + 2];
+        eta.p<T>()[k] = out[k * 4 + 3];
+    }
+    for (Vec *w : {&theta, &phi, &psi, &eta}) {
+        w->init = true;
+        w->zero = false;
+    }
+    r.zero = false;
+}
+
+// blas_merged_rbicgstab.inl:120-193: x += alpha_conv v_ + omega_conv t_;
+// z = t_ - omega z; v_ = z + beta v_ - beta omega s
+template <typename T>
+void merged_rbicgstab_group2(Vec &x, Vec &v_, Vec &t_, Vec &z, Vec &s, const Vec &alpha_conv,
+                             const Vec &omega_conv, const Vec &omega, const Vec &beta) {
+    if (x.zero) set_const<T>(x, 0.0, true);
+    if (v_.zero) set_const<T>(v_, 0.0, true);
+    if (t_.zero) forced_set_const<T>(t_, 0.0);
+    if (z.zero) set_const<T>(z, 0.0, true);
+    if (s.zero) forced_set_const<T>(s, 0.0);
+    const int NV = x.nv;
+    T *xp = x.p<T>(), *vp = v_.p<T>(), *zp = z.p<T>();
+    const T *tp = t_.p<T>(), *sp = s.p<T>();
+    const T *ac = alpha_conv.p<T>(), *oc = omega_conv.p<T>(), *om = omega.p<T>(),
+            *be = beta.p<T>();
+    for (uint64_t i = 0; i < NV * x.size; i += NV)
+        for (int k = 0; k < NV; ++k) {
+            xp[i + k] += ac[k] * vp[i + k] + oc[k] * tp[i + k];
+            zp[i + k] = tp[i + k] - om[k] * zp[i + k];
+            vp[i + k] = zp[i + k] + be[k] * vp[i + k] - be[k] * om[k] * sp[i + k];
+        }
+    x.zero = z.zero = v_.zero = false;
+}
+
 template <typename T>
 void merged_jacobi(Vec &x, const Vec &b, const Vec &inv_diag, Vec &r, const Vec &relax) {
     if (x.empty()) {
@@ -1756,6 +1817,87 @@ static void solve_pcg(Solver &S, Vec &x, Vec &b, const Vec &conv) {
     } while (it < S.sp.max_iters);
 }
 
+// rbicgstab.inl:44-243 (merged = false) and merged_rbicgstab.inl:44-230
+// (merged = true): BiCGStab reordered so that each preconditioner application
+// can overlap a reduction
+static void solve_rbicgstab(Solver &S, Vec &x, Vec &b, const Vec &conv, bool merged) {
+    typedef double F;
+    const int NV = S.NV;
+    reset_stats(S);
+    int &it = S.st.iters;
+    Vec iconv = conv;
+    Vec a1 = typed_scalar<F>(NV, 1.0), a_1 = typed_scalar<F>(NV, -1.0);
+    Vec rho = make_vec<F>(1, NV), rho0 = make_vec<F>(1, NV), res = make_vec<F>(1, NV);
+    Vec theta = make_vec<F>(1, NV), phi = make_vec<F>(1, NV), psi = make_vec<F>(1, NV),
+        delta = make_vec<F>(1, NV), alpha = make_vec<F>(1, NV), beta = make_vec<F>(1, NV),
+        omega = make_vec<F>(1, NV), eta = make_vec<F>(1, NV), temp = make_vec<F>(1, NV);
+    Vec alpha_conv = make_vec<F>(1, NV), omega_conv = make_vec<F>(1, NV);
+    for (auto &v : S.buf) blas::set_const<F>(v, 0.0);
+    Vec &r0 = S.buf[0], &r = S.buf[1], &z = S.buf[2], &v_ = S.buf[3], &v = S.buf[4],
+        &s = S.buf[5], &t_ = S.buf[6], &t = S.buf[7];
+    get_residual<F>(S, x, b, r0, rho0, true);
+    blas::copy<F>(r0, r);
+    if (converged<F>(S, rho0, rho0, iconv)) return;
+    blas::copy<F>(rho0, rho);
+    blas::set_const<F>(z, 0.0);
+    precond_apply(S, z, r0);
+    blas::copy<F>(z, v_);
+    do {
+        ++it;
+        blas2::Ax_y<F>(*S.A, v_, v);
+        blas::dot<F>(v, r0, delta);
+        blas::set_const<F>(s, 0.0);
+        precond_apply(S, s, v);
+        blas::xdivy_z<F>(rho, delta, alpha);
+        blas::scal<F>(a_1, alpha);
+        blas::axpby_z<F>(a1, z, alpha, s, t_);
+        blas::scal<F>(a_1, alpha);
+        blas2::Ax_y<F>(*S.A, t_, t);
+        if (merged) {
+            blas::merged_rbicgstab_group1<F>(r, v, t, r0, alpha, theta, phi, psi, eta);
+        } else {
+            blas::scal<F>(a_1, alpha);
+            blas::axpby<F>(alpha, v, a1, r);
+            blas::scal<F>(a_1, alpha);
+            blas::dot<F>(t, r, theta);
+            blas::dot<F>(t, t, phi);
+            blas::dot<F>(t, r0, psi);
+            blas::dot<F>(r, r, eta);
+        }
+        blas::set_const<F>(z, 0.0);
+        precond_apply(S, z, t);
+        blas::xdivy_z<F>(theta, phi, omega);
+        blas::scal<F>(a_1, omega);
+        blas::axpby<F>(omega, t, a1, r);
+        blas::scal<F>(a_1, omega);
+        blas::ax_y<F>(omega, theta, res);
+        blas::axpby<F>(a1, eta, a_1, res);
+        blas::ax_y<F>(iconv, alpha, alpha_conv);
+        blas::ax_y<F>(iconv, omega, omega_conv);
+        if (!merged) blas::axpbypcz<F>(alpha_conv, v_, omega_conv, t_, a1, x);
+        if (converged<F>(S, res, rho0, iconv)) {
+            if (merged) blas::axpbypcz<F>(alpha_conv, v_, omega_conv, t_, a1, x);
+            return;
+        }
+        blas::ax_y<F>(omega, psi, rho);
+        blas::scal<F>(a_1, rho);
+        blas::ax_y<F>(delta, omega, temp);
+        blas::xdivy_z<F>(rho, temp, beta);
+        if (merged) {
+            blas::ax_y<F>(iconv, alpha, alpha_conv);
+            blas::ax_y<F>(iconv, omega, omega_conv);
+            blas::merged_rbicgstab_group2<F>(x, v_, t_, z, s, alpha_conv, omega_conv, omega,
+                                             beta);
+        } else {
+            blas::scal<F>(a_1, omega);
+            blas::axpby<F>(a1, t_, omega, z);
+            blas::ax_y<F>(omega, beta, delta);
+            blas::scal<F>(a_1, omega);
+            blas::axpbypcz<F>(a1, z, delta, s, beta, v_);
+        }
+    } while (it < S.sp.max_iters);
+}
+
 template <typename T>
 static void solve(Solver &S, Vec &x, Vec &b, const Vec &conv) {
     const std::string &m = S.method;
@@ -1781,6 +1923,10 @@ static void solve(Solver &S, Vec &x, Vec &b, const Vec &conv) {
         solve_bicgstab(S, x, b, conv, true);
     else if (m == "PCG")
         solve_pcg(S, x, b, conv);
+    else if (m == "RBiCGStab")
+        solve_rbicgstab(S, x, b, conv, false);
+    else if (m == "MergedRBiCGStab")
+        solve_rbicgstab(S, x, b, conv, true);
 }
 
 // ----------------------------------------------------------------------------
@@ -1803,6 +1949,7 @@ static int buffer_nvecs(const std::string &m) {
     if (m == "MultiGrid") return 1;
     if (m == "BiCGStab") return 6;
     if (m == "PCG") return 4;
+    if (m == "RBiCGStab" || m == "MergedRBiCGStab") return 8;
     if (m == "PBiCGStab" || m == "MergedBiCGStab" || m == "MergedPBiCGStab") return 8;
     return 0;
 }

@@ -83,6 +83,7 @@ enum Sc : int {
     SC_OMEGA_C,
     SC_NSCAL,  // -(omega*beta), the v coefficient of the p update
     SC_RELAX,
+    SC_ETA,    // (r, r) of the reordered BiCGStab
     SC_COUNT
 };
 constexpr int SC_STRIDE = 32;
@@ -99,7 +100,7 @@ inline int canon_blocks(uint64_t n, int nv) {
 // Canonical reduction: block partials, then the last block finishes.
 // ---------------------------------------------------------------------------
 struct RedArgs {
-    void *part;              // [BMAX][32][3] partial sums (element type of the kernel)
+    void *part;              // [BMAX][32][4] partial sums (element type of the kernel)
     unsigned *ticket;        // zero between launches
     unsigned *flag = nullptr;  // bit 0: a bounded wait ran out (read by the host)
 };
@@ -942,6 +943,129 @@ struct OpPcgP {
     __device__ void operator()(uint64_t e) const {
         const int k = (int)(e % nv);
         p[e] = add(mul(1.0, z[e]), mul(sc[SC_BETA * SC_STRIDE + k], p[e]));
+    }
+};
+
+// Reordered BiCGStab (rbicgstab.inl:44-243, merged_rbicgstab.inl:44-230).
+// merged_rbicgstab_group1 (blas_merged_rbicgstab.inl:33-116): r = r - alpha v,
+// then theta = (t, r), phi = (t, t), psi = (t, r0), eta = (r, r). The
+// unmerged form's r = (-alpha) v + 1 r is the same value bit for bit.
+// Finaliser: omega = theta / phi; res = 1 eta + (-1)(omega theta);
+// alpha_conv, omega_conv; rho = -(omega psi); beta = rho / (delta omega),
+// delta = (v, r0) in SC_SCAL1.
+template <int NV>
+struct ERbGroup1 {
+    double *r;
+    const double *v, *t, *r0;
+    double *sc;
+    template <int NR>
+    __device__ void elem(uint64_t i, int k, double (&acc)[NR]) const {
+        const uint64_t e = i * NV + k;
+        const double rv = sub(r[e], mul(sc[SC_ALPHA * SC_STRIDE + k], v[e]));
+        r[e] = rv;
+        const double tv = t[e];
+        acc[0] = add(acc[0], mul(tv, rv));
+        acc[1] = add(acc[1], mul(tv, tv));
+        acc[2] = add(acc[2], mul(tv, r0[e]));
+        acc[3] = add(acc[3], mul(rv, rv));
+    }
+    __device__ void operator()(int k, const double *s4) const {
+        double *S = sc;
+        const double theta = s4[0], phi = s4[1], psi = s4[2], eta = s4[3];
+        S[SC_THETA * SC_STRIDE + k] = theta;
+        S[SC_PHI * SC_STRIDE + k] = phi;
+        S[SC_PSI * SC_STRIDE + k] = psi;
+        S[SC_ETA * SC_STRIDE + k] = eta;
+        const double omega = dvd(theta, phi);
+        S[SC_OMEGA * SC_STRIDE + k] = omega;
+        S[SC_RES * SC_STRIDE + k] = add(mul(1.0, eta), mul(-1.0, mul(omega, theta)));
+        const double ic = S[SC_ICONV * SC_STRIDE + k];
+        S[SC_ALPHA_C * SC_STRIDE + k] = mul(ic, S[SC_ALPHA * SC_STRIDE + k]);
+        S[SC_OMEGA_C * SC_STRIDE + k] = mul(ic, omega);
+        const double rho = mul(-1.0, mul(omega, psi));
+        S[SC_RHO * SC_STRIDE + k] = rho;
+        S[SC_BETA * SC_STRIDE + k] = dvd(rho, mul(S[SC_SCAL1 * SC_STRIDE + k], omega));
+    }
+};
+
+// t_ = 1 z + (-alpha) s  (axpby_z, blas_ext.inl:193-239, with its zero-flag
+// branches)
+struct OpRbT {
+    double *t_;
+    const double *z, *s, *sc;
+    int nv;
+    bool z_zero, s_zero;
+    __device__ void operator()(uint64_t e) const {
+        const int k = (int)(e % nv);
+        const double na = mul(-1.0, sc[SC_ALPHA * SC_STRIDE + k]);
+        t_[e] = z_zero ? mul(na, s[e]) : s_zero ? mul(1.0, z[e]) : add(mul(1.0, z[e]), mul(na, s[e]));
+    }
+};
+
+// x = alpha_conv v_ + omega_conv t_ + 1 x (axpbypcz; x zero-flagged: without
+// the x term)
+__device__ __forceinline__ double rb_x(double ac, double v, double oc, double t, double x,
+                                       bool x_zero) {
+    return x_zero ? add(mul(ac, v), mul(oc, t)) : add(add(mul(ac, v), mul(oc, t)), mul(1.0, x));
+}
+
+// r = (-omega) t + 1 r; with x: the unmerged form's x update before the
+// convergence test (rbicgstab.inl:200-205)
+struct OpRbR {
+    double *r, *x;
+    const double *t, *v_, *t_, *sc;
+    int nv;
+    bool x_zero;
+    __device__ void operator()(uint64_t e) const {
+        const int k = (int)(e % nv);
+        r[e] = add(mul(mul(-1.0, sc[SC_OMEGA * SC_STRIDE + k]), t[e]), mul(1.0, r[e]));
+        if (x)
+            x[e] = rb_x(sc[SC_ALPHA_C * SC_STRIDE + k], v_[e], sc[SC_OMEGA_C * SC_STRIDE + k],
+                        t_[e], x[e], x_zero);
+    }
+};
+
+// the merged form's x update on convergence (merged_rbicgstab.inl:199-203)
+struct OpRbX {
+    double *x;
+    const double *v_, *t_, *sc;
+    int nv;
+    bool x_zero;
+    __device__ void operator()(uint64_t e) const {
+        const int k = (int)(e % nv);
+        x[e] = rb_x(sc[SC_ALPHA_C * SC_STRIDE + k], v_[e], sc[SC_OMEGA_C * SC_STRIDE + k], t_[e],
+                    x[e], x_zero);
+    }
+};
+
+// Merged: merged_rbicgstab_group2 (blas_merged_rbicgstab.inl:120-193) with
+// alpha_conv, omega_conv taken with the updated iconv:
+//   x = x + (ac v_ + oc t_); z = t_ - omega z; v_ = (z + beta v_) - (beta omega) s.
+// Unmerged (rbicgstab.inl:226-236): z = 1 t_ + (-omega) z;
+//   v_ = (1 z + ((-omega) beta) s) + beta v_.
+struct OpRbG2 {
+    double *x, *v_, *z;
+    const double *t_, *s, *sc;
+    int nv;
+    bool merged, x_zero;
+    __device__ void operator()(uint64_t e) const {
+        const int k = (int)(e % nv);
+        const double om = sc[SC_OMEGA * SC_STRIDE + k], be = sc[SC_BETA * SC_STRIDE + k];
+        const double tv = t_[e];
+        if (merged) {
+            const double ic = sc[SC_ICONV * SC_STRIDE + k];
+            const double ac = mul(ic, sc[SC_ALPHA * SC_STRIDE + k]), oc = mul(ic, om);
+            const double xo = x_zero ? 0.0 : x[e];
+            x[e] = add(xo, add(mul(ac, v_[e]), mul(oc, tv)));
+            const double zn = sub(tv, mul(om, z[e]));
+            z[e] = zn;
+            v_[e] = sub(add(zn, mul(be, v_[e])), mul(mul(be, om), s[e]));
+        } else {
+            const double nom = mul(-1.0, om);
+            const double zn = add(mul(1.0, tv), mul(nom, z[e]));
+            z[e] = zn;
+            v_[e] = add(add(mul(1.0, zn), mul(mul(nom, be), s[e])), mul(be, v_[e]));
+        }
     }
 };
 

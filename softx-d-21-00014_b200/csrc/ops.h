@@ -45,6 +45,17 @@ void pcg_dots(uint64_t n, const double *r, const double *z, double *sc, bool fir
 void pcg_xr(uint64_t n, double *x, double *r, const double *p, const double *Ap,
             const double *sc, bool x_zero, int nv, cudaStream_t s);
 void pcg_p(uint64_t n, double *p, const double *z, const double *sc, int nv, cudaStream_t s);
+// Reordered BiCGStab (rbicgstab.inl, merged_rbicgstab.inl)
+void rb_group1(uint64_t n, double *r, const double *v, const double *t, const double *r0,
+               double *sc, int nv, cudaStream_t s);
+void rb_t(uint64_t n, double *t_, const double *z, const double *s_, const double *sc, bool z_zero,
+          bool s_zero, int nv, cudaStream_t s);
+void rb_r(uint64_t n, double *r, double *x, const double *t, const double *v_, const double *t_,
+          const double *sc, bool x_zero, int nv, cudaStream_t s);
+void rb_x(uint64_t n, double *x, const double *v_, const double *t_, const double *sc,
+          bool x_zero, int nv, cudaStream_t s);
+void rb_group2(uint64_t n, double *x, double *v_, double *z, const double *t_, const double *s_,
+               const double *sc, bool merged, bool x_zero, int nv, cudaStream_t s);
 void spmv_dot3(const DCsr &A, const double *sa, double *t, const double *s_, double *sc, int nv,
                cudaStream_t s);
 

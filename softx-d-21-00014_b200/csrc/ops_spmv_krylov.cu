@@ -61,6 +61,14 @@ void pcg_dots(uint64_t n, const double *r, const double *z, double *sc, bool fir
     });
 }
 
+void rb_group1(uint64_t n, double *r, const double *v, const double *t, const double *r0,
+               double *sc, int nv, cudaStream_t s) {
+    dispatch_nv(nv, [&](auto nvc) {
+        constexpr int NV = decltype(nvc)::value;
+        launch_rows<double, NV, 4>(n, k::ERbGroup1<NV>{r, v, t, r0, sc}, s);
+    });
+}
+
 void spmv_dot3(const DCsr &A, const double *sa, double *t, const double *s_, double *sc, int nv,
                cudaStream_t s) {
     XG_DISPATCH(A, nv, { launch<double, double, I, NV, 3>(A, sa, k::EDot3<NV>{t, s_, sc}, s); });

@@ -28,7 +28,7 @@ void Ctx::init() {
     XG_CUDA(cudaGetDevice(&device));
     XG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     XG_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-    red_part.alloc((size_t)k::BMAX * 32 * 3 * sizeof(double));
+    red_part.alloc((size_t)k::BMAX * 32 * 4 * sizeof(double));
     red_ticket.alloc(sizeof(unsigned) * 4);
     red_out.alloc(128 * sizeof(double));
     XG_CUDA(cudaMemsetAsync(red_ticket.p, 0, red_ticket.bytes, stream));
@@ -92,6 +92,22 @@ void pcg_xr(uint64_t n, double *x, double *r, const double *p, const double *Ap,
 }
 void pcg_p(uint64_t n, double *p, const double *z, const double *sc, int nv, cudaStream_t s) {
     flat(n * nv, k::OpPcgP{p, z, sc, nv}, s);
+}
+void rb_t(uint64_t n, double *t_, const double *z, const double *s_, const double *sc, bool z_zero,
+          bool s_zero, int nv, cudaStream_t s) {
+    flat(n * nv, k::OpRbT{t_, z, s_, sc, nv, z_zero, s_zero}, s);
+}
+void rb_r(uint64_t n, double *r, double *x, const double *t, const double *v_, const double *t_,
+          const double *sc, bool x_zero, int nv, cudaStream_t s) {
+    flat(n * nv, k::OpRbR{r, x, t, v_, t_, sc, nv, x_zero}, s);
+}
+void rb_x(uint64_t n, double *x, const double *v_, const double *t_, const double *sc,
+          bool x_zero, int nv, cudaStream_t s) {
+    flat(n * nv, k::OpRbX{x, v_, t_, sc, nv, x_zero}, s);
+}
+void rb_group2(uint64_t n, double *x, double *v_, double *z, const double *t_, const double *s_,
+               const double *sc, bool merged, bool x_zero, int nv, cudaStream_t s) {
+    flat(n * nv, k::OpRbG2{x, v_, z, t_, s_, sc, nv, merged, x_zero}, s);
 }
 void group5(uint64_t n, double *x, double *p, const double *s_, const double *r, const double *v,
             const double *sc, int nv, cudaStream_t s) {

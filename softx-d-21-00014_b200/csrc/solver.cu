@@ -766,10 +766,78 @@ void Krylov::solve_pcg(DVec &x, DVec &b, const std::vector<double> &conv) {
     XG_CUDA(cudaStreamSynchronize(s));
 }
 
+// rbicgstab.inl:44-243 (rb_merged = false), merged_rbicgstab.inl:44-230
+// (true). Kernels: v = A v_ with delta = (v, r0) and alpha; s = M^-1 v;
+// t_ = z - alpha s; t = A t_; group 1 (r update, four dots, the scalar
+// recurrences); z = M^-1 t; r = r - omega t (with the unmerged x update);
+// convergence test; group 2.
+void Krylov::solve_rbicgstab(DVec &x, DVec &b, const std::vector<double> &conv) {
+    cudaStream_t s = S();
+    std::vector<double> iconv = conv;
+    upload_iconv(iconv);
+    double *SC = sc.as<double>();
+    for (auto &v : buf) {
+        v.zero = true;
+        v.init = true;
+    }
+    DVec &r0 = buf[0], &r = buf[1], &z = buf[2], &v_ = buf[3], &v = buf[4], &s_ = buf[5],
+         &t_ = buf[6], &t = buf[7];
+    std::vector<double> rho0(NV), res(NV);
+    residual_norm<double>(*A, x, b, r0, NV, rho0.data());
+    // copy(r0, r); rho = rho0
+    ops::convert<double, double>(r.p<double>(), r0.p<double>(), r.elems(), s);
+    r.zero = false;
+    if (check(rho0.data(), rho0.data(), iconv)) return;
+    XG_CUDA(cudaMemcpyAsync(SC + k::SC_RHO * k::SC_STRIDE, ctx().red_out.as<double>(),
+                            NV * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    apply_M(z, r0);
+    v_.zero = z.zero;
+    if (!z.zero) ops::convert<double, double>(v_.p<double>(), z.p<double>(), v_.elems(), s);
+    do {
+        ++st.iters;
+        ops::spmv_dot_alpha(*A, v_.p<double>(), v.p<double>(), r0.p<double>(), SC, NV, s);
+        v.zero = false;
+        apply_M(s_, v);
+        ops::rb_t(n, t_.p<double>(), z.p<double>(), s_.p<double>(), SC, z.zero, s_.zero, NV, s);
+        t_.zero = false;
+        ops::spmv<double>(*A, t_.p<double>(), t.p<double>(), NV, false, s);
+        t.zero = false;
+        ops::rb_group1(n, r.p<double>(), v.p<double>(), t.p<double>(), r0.p<double>(), SC, NV, s);
+        apply_M(z, t);
+        ops::rb_r(n, r.p<double>(), rb_merged ? nullptr : x.p<double>(), t.p<double>(),
+                  v_.p<double>(), t_.p<double>(), SC, x.zero, NV, s);
+        if (!rb_merged) {
+            x.zero = false;
+            x.init = true;
+        }
+        read_scalars(SC + k::SC_RES * k::SC_STRIDE, res.data(), NV);
+        if (check(res.data(), rho0.data(), iconv)) {
+            if (rb_merged) {
+                ops::rb_x(n, x.p<double>(), v_.p<double>(), t_.p<double>(), SC, x.zero, NV, s);
+                x.zero = false;
+                x.init = true;
+            }
+            return;
+        }
+        ops::rb_group2(n, x.p<double>(), v_.p<double>(), z.p<double>(), t_.p<double>(),
+                       s_.p<double>(), SC, rb_merged, x.zero, NV, s);
+        z.zero = v_.zero = false;
+        if (rb_merged) {
+            x.zero = false;
+            x.init = true;
+        }
+    } while (st.iters < cfg.max_iters);
+    XG_CUDA(cudaStreamSynchronize(s));
+}
+
 void Krylov::solve(DVec &x, DVec &b, const std::vector<double> &conv) {
     reset_stats();
     if (pcg) {
         solve_pcg(x, b, conv);
+        return;
+    }
+    if (rbicgstab) {
+        solve_rbicgstab(x, b, conv);
         return;
     }
     cudaStream_t s = S();
@@ -863,7 +931,7 @@ void SolverHierarchy::build(const Params &P, const HCsr &hA_, const DCsr *A_, in
         return;
     }
     if (m == "MergedPBiCGStab" || m == "PBiCGStab" || m == "MergedBiCGStab" || m == "BiCGStab" ||
-        m == "PCG") {
+        m == "PCG" || m == "RBiCGStab" || m == "MergedRBiCGStab") {
         auto *kr = new Krylov();
         kr->cfg = c;
         kr->role = "solver";
@@ -872,8 +940,11 @@ void SolverHierarchy::build(const Params &P, const HCsr &hA_, const DCsr *A_, in
         kr->n = hA.nrows;
         kr->precond_form = (m != "MergedBiCGStab");
         kr->pcg = (m == "PCG");
+        kr->rbicgstab = (m == "RBiCGStab" || m == "MergedRBiCGStab");
+        kr->rb_merged = (m == "MergedRBiCGStab");
         kr->setup();
-        const bool wants_M = (m == "MergedPBiCGStab" || m == "PBiCGStab" || m == "PCG");
+        const bool wants_M = (m == "MergedPBiCGStab" || m == "PBiCGStab" || m == "PCG" ||
+                              kr->rbicgstab);
         if (wants_M && P.has("preconditioner")) {
             SolverCfg pc = resolve_cfg(P.get("preconditioner"), "preconditioner");
             if (pc.method == "MultiGrid") {

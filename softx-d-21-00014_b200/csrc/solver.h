@@ -93,6 +93,8 @@ class Krylov : public SolverBase {
   public:
     bool precond_form = true;  // (P)BiCGStab structure; false: MergedBiCGStab
     bool pcg = false;          // preconditioned conjugate gradients (pcg.inl)
+    bool rbicgstab = false;    // reordered BiCGStab (rbicgstab.inl)
+    bool rb_merged = false;    // ... in its merged form (merged_rbicgstab.inl)
     std::unique_ptr<SolverBase> M;
     DevBuf sc;                 // scalar block (kernels.cuh Sc)
     void setup() override;
@@ -104,6 +106,7 @@ class Krylov : public SolverBase {
     void apply_M(DVec &out, DVec &in);
     void run_M(DVec &out, DVec &in);
     void solve_pcg(DVec &x, DVec &b, const std::vector<double> &conv);
+    void solve_rbicgstab(DVec &x, DVec &b, const std::vector<double> &conv);
     void upload_iconv(const std::vector<double> &iconv);
     std::map<std::tuple<const void *, const void *, bool>, MGraph> graphs_;
 };

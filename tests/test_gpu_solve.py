@@ -93,13 +93,14 @@ def test_config1_merged_pbicgstab_jacobi(gpu, oracle):
     assert S.level_info(0, 0)["col_bytes"] == 2
 
 
-@pytest.mark.parametrize("method", ["PBiCGStab", "BiCGStab", "MergedBiCGStab", "PCG"])
+@pytest.mark.parametrize("method", ["PBiCGStab", "BiCGStab", "MergedBiCGStab", "PCG",
+                                    "RBiCGStab", "MergedRBiCGStab"])
 @pytest.mark.parametrize("nv", [2, 8])
 def test_krylov_variants(gpu, oracle, method, nv):
     row, col, val = gpu.generate_cube(14, 13, 12)
     params = {"solver": {"method": method, "max_iters": 500, "rel_tolerance": 1e-9,
                          "abs_tolerance": 0}}
-    if method in ("PBiCGStab", "PCG"):
+    if method in ("PBiCGStab", "PCG", "RBiCGStab", "MergedRBiCGStab"):
         params["preconditioner"] = {"method": "Jacobi", "max_iters": 3}
     check(gpu, oracle, row, col, val, nv, params, seed=nv, tol=1e-9)
 
@@ -258,3 +259,19 @@ def test_graph_replay_matches_direct_launches(gpu, smoother):
     assert s0["iters"] == s1["iters"] and s0["iters"] >= 3
     assert x0.tobytes() == x1.tobytes()
     assert l0 == l1
+
+
+@pytest.mark.parametrize("method", ["RBiCGStab", "MergedRBiCGStab"])
+def test_rbicgstab_with_amg(gpu, oracle, method):
+    """Reordered BiCGStab (rbicgstab.inl, merged_rbicgstab.inl) with an FP32
+    AMG V-cycle as the preconditioner, three applications graph-replayed."""
+    row, col, val = gpu.generate_diffusion(27, 14, 13, 12, 1.0, 1.0, 7)
+    nv = 8
+    params = {"solver": {"method": method, "max_iters": 100, "rel_tolerance": 1e-8,
+                         "abs_tolerance": 0, "gpu_index_compress": 2},
+              "preconditioner": dict(MG_BASE, method="MultiGrid", gpu_precond_f32=1,
+                                     gpu_index_compress=2),
+              "pre_smoother": {"method": "Chebyshev"}, "post_smoother": {"method": "Chebyshev"},
+              "coarse_grid_solver": {"method": "Direct"}}
+    st, S = check(gpu, oracle, row, col, val, nv, params, seed=8)
+    assert st["iters"] < 30
