@@ -175,6 +175,17 @@ int XAMG_b200_write_system(const char *path, uint32_t nrows, uint32_t nnz, const
 int XAMG_b200_solver_hierarchy_save(size_t sid, const char *path);
 int XAMG_b200_matrix_hierarchy_load(size_t mid, const char *path);
 
+/* Dense BF16 GEMM on the tcgen05 tensor cores with FP32 accumulation (no
+ * counterpart: the dense layers of the learned coarse initial guess).
+ * C[M][N] = A[M][K] * B[N][K]^T; A, B row-major BF16 on the device, C with
+ * row stride ldc. mode 0: C FP32 = acc (+ bias[N] if not NULL); 1: C BF16 =
+ * acc (+ bias); 2: C BF16 = max(acc + bias, 0); 3: C BF16 = acc where
+ * aux[M][ld_aux] (BF16) > 0, else 0. M and N multiples of 128, K a multiple
+ * of 64, pointers 16-byte aligned. */
+int XAMG_b200_gemm_bf16(uint64_t M, uint64_t N, uint64_t K, const void *A, const void *B,
+                        void *C, uint64_t ldc, int mode, const float *bias, const void *aux,
+                        uint64_t ld_aux, void *stream);
+
 /* y = A x (mode 0) or y += A x (mode 1) with level matrix `which` of a
  * solver, as its solves run it: on the library's own copy, with the x-staging
  * plan it has for nv (no counterpart; the kernel-level view of the solver's

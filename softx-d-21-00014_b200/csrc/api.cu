@@ -907,6 +907,14 @@ int XAMG_b200_matrix_hierarchy_load(XAMG_matrix_id mid, const char *path) {
     });
 }
 
+int XAMG_b200_gemm_bf16(uint64_t M, uint64_t N, uint64_t K, const void *A, const void *B,
+                        void *C, uint64_t ldc, int mode, const float *bias, const void *aux,
+                        uint64_t ld_aux, void *stream) {
+    return guarded([&] {
+        ops::mm::gemm_bf16(M, N, K, A, B, C, ldc, mode, bias, aux, ld_aux, pick(stream));
+    });
+}
+
 int XAMG_b200_solver_level_spmv(size_t sid, int level, int which, const void *x, void *y, int nv,
                                 int mode, void *stream) {
     return guarded([&] {

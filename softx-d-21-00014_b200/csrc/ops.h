@@ -56,6 +56,15 @@ void rb_x(uint64_t n, double *x, const double *v_, const double *t_, const doubl
           bool x_zero, int nv, cudaStream_t s);
 void rb_group2(uint64_t n, double *x, double *v_, double *z, const double *t_, const double *s_,
                const double *sc, bool merged, bool x_zero, int nv, cudaStream_t s);
+namespace mm {
+// C[M][N] = A[M][K] * B[N][K]^T in BF16 with FP32 accumulation on the
+// tcgen05 tensor cores (gemm.cu); mode 0 FP32 out (+ bias), 1 BF16 out
+// (+ bias), 2 BF16 ReLU(acc + bias), 3 BF16 acc masked by aux > 0.
+void gemm_bf16(uint64_t M, uint64_t N, uint64_t K, const void *A, const void *B, void *C,
+               uint64_t ldc, int mode, const float *bias, const void *aux, uint64_t ld_aux,
+               cudaStream_t s);
+}  // namespace mm
+
 void spmv_dot3(const DCsr &A, const double *sa, double *t, const double *s_, double *sc, int nv,
                cudaStream_t s);
 

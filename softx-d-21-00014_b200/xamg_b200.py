@@ -57,7 +57,7 @@ EXT_SYMBOLS = [
     "XAMG_b200_set_device", "XAMG_b200_dot_noalloc", "XAMG_b200_wait_selftest",
     "XAMG_b200_solver_level_spmv", "XAMG_b200_read_system_size", "XAMG_b200_read_system",
     "XAMG_b200_write_system", "XAMG_b200_solver_hierarchy_save",
-    "XAMG_b200_matrix_hierarchy_load",
+    "XAMG_b200_matrix_hierarchy_load", "XAMG_b200_gemm_bf16",
 ]
 
 
@@ -181,6 +181,8 @@ def lib():
         "XAMG_b200_write_system": (C.c_int, [C.c_char_p, C.c_uint32, C.c_uint32, vp, vp, vp,
                                              C.c_uint16, vp, vp]),
         "XAMG_b200_solver_hierarchy_save": (C.c_int, [C.c_size_t, C.c_char_p]),
+        "XAMG_b200_gemm_bf16": (C.c_int, [u64, u64, u64, vp, vp, vp, u64, C.c_int, vp, vp, u64,
+                                          vp]),
         "XAMG_b200_matrix_hierarchy_load": (C.c_int, [C.c_size_t, C.c_char_p]),
     }
     for name, (res, args) in sig.items():
