@@ -186,6 +186,23 @@ int XAMG_b200_gemm_bf16(uint64_t M, uint64_t N, uint64_t K, const void *A, const
                         void *C, uint64_t ldc, int mode, const float *bias, const void *aux,
                         uint64_t ld_aux, void *stream);
 
+/* The MLP of the learned coarse initial guess (no counterpart): n_in -> h ->
+ * h -> n_out dense layers with ReLU, BF16 weights and activations on the
+ * tcgen05 GEMM with FP32 accumulation, FP32 master weights trained by Adam on
+ * the mean squared error. Widths and batches are multiples of 128. X, T, Y
+ * are FP32 device arrays [batch][n_in] / [batch][n_out]. Parameters (and
+ * gradients) are laid out W1^T [h][n_in], b1 [h], W2^T [h][h], b2 [h],
+ * W3^T [n_out][h], b3 [n_out] in host FP32 arrays of *count values. */
+int XAMG_b200_mlp_create(uint32_t n_in, uint32_t n_hidden, uint32_t n_out, uint64_t seed,
+                         size_t *id);
+int XAMG_b200_mlp_destroy(size_t id);
+int XAMG_b200_mlp_predict(size_t id, uint32_t batch, const float *X, float *Y);
+int XAMG_b200_mlp_train_step(size_t id, uint32_t batch, const float *X, const float *T, float lr,
+                             double *loss);
+int XAMG_b200_mlp_gradients(size_t id, uint32_t batch, const float *X, const float *T,
+                            float *grads, double *loss);
+int XAMG_b200_mlp_params(size_t id, float *params, int set, uint64_t *count);
+
 /* y = A x (mode 0) or y += A x (mode 1) with level matrix `which` of a
  * solver, as its solves run it: on the library's own copy, with the x-staging
  * plan it has for nv (no counterpart; the kernel-level view of the solver's

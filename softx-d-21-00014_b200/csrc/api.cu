@@ -15,6 +15,7 @@
 #include "../../include/xamg_c_api.h"
 #include "ops.h"
 #include "io.h"
+#include "mlp.h"
 #include "solver.h"
 
 #ifndef XAMG_NV
@@ -912,6 +913,64 @@ int XAMG_b200_gemm_bf16(uint64_t M, uint64_t N, uint64_t K, const void *A, const
                         uint64_t ld_aux, void *stream) {
     return guarded([&] {
         ops::mm::gemm_bf16(M, N, K, A, B, C, ldc, mode, bias, aux, ld_aux, pick(stream));
+    });
+}
+
+static std::vector<std::unique_ptr<Mlp>> g_mlps;
+
+int XAMG_b200_mlp_create(uint32_t n_in, uint32_t n_hidden, uint32_t n_out, uint64_t seed,
+                         size_t *id) {
+    return guarded([&] {
+        XG_REQUIRE(id, XAMG_ERR_INVALID_ARG, "null id");
+        std::unique_ptr<Mlp> m(new Mlp());
+        m->init(n_in, n_hidden, n_out, seed);
+        g_mlps.push_back(std::move(m));
+        *id = g_mlps.size() - 1;
+    });
+}
+
+int XAMG_b200_mlp_destroy(size_t id) {
+    return guarded([&] {
+        get(g_mlps, id, "mlp");
+        XG_CUDA(cudaStreamSynchronize(ctx().stream));
+        g_mlps[id].reset();
+    });
+}
+
+int XAMG_b200_mlp_predict(size_t id, uint32_t batch, const float *X, float *Y) {
+    return guarded([&] {
+        XG_REQUIRE(X && Y, XAMG_ERR_INVALID_ARG, "null argument");
+        get(g_mlps, id, "mlp").forward(batch, X, Y);
+    });
+}
+
+int XAMG_b200_mlp_train_step(size_t id, uint32_t batch, const float *X, const float *T, float lr,
+                             double *loss) {
+    return guarded([&] {
+        XG_REQUIRE(X && T, XAMG_ERR_INVALID_ARG, "null argument");
+        const double l = get(g_mlps, id, "mlp").train_step(batch, X, T, lr);
+        if (loss) *loss = l;
+        ctx().check_flags();
+    });
+}
+
+int XAMG_b200_mlp_gradients(size_t id, uint32_t batch, const float *X, const float *T,
+                            float *grads, double *loss) {
+    return guarded([&] {
+        XG_REQUIRE(X && T && grads, XAMG_ERR_INVALID_ARG, "null argument");
+        Mlp &m = get(g_mlps, id, "mlp");
+        const double l = m.gradients(batch, X, T);
+        m.copy_params(grads, false, true);
+        if (loss) *loss = l;
+        ctx().check_flags();
+    });
+}
+
+int XAMG_b200_mlp_params(size_t id, float *params, int set, uint64_t *count) {
+    return guarded([&] {
+        Mlp &m = get(g_mlps, id, "mlp");
+        if (count) *count = m.param_count();
+        if (params) m.copy_params(params, set != 0, false);
     });
 }
 

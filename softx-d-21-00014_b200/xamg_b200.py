@@ -57,7 +57,9 @@ EXT_SYMBOLS = [
     "XAMG_b200_set_device", "XAMG_b200_dot_noalloc", "XAMG_b200_wait_selftest",
     "XAMG_b200_solver_level_spmv", "XAMG_b200_read_system_size", "XAMG_b200_read_system",
     "XAMG_b200_write_system", "XAMG_b200_solver_hierarchy_save",
-    "XAMG_b200_matrix_hierarchy_load", "XAMG_b200_gemm_bf16",
+    "XAMG_b200_matrix_hierarchy_load", "XAMG_b200_gemm_bf16", "XAMG_b200_mlp_create",
+    "XAMG_b200_mlp_destroy", "XAMG_b200_mlp_predict", "XAMG_b200_mlp_train_step",
+    "XAMG_b200_mlp_gradients", "XAMG_b200_mlp_params",
 ]
 
 
@@ -183,6 +185,15 @@ def lib():
         "XAMG_b200_solver_hierarchy_save": (C.c_int, [C.c_size_t, C.c_char_p]),
         "XAMG_b200_gemm_bf16": (C.c_int, [u64, u64, u64, vp, vp, vp, u64, C.c_int, vp, vp, u64,
                                           vp]),
+        "XAMG_b200_mlp_create": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, u64,
+                                           C.POINTER(C.c_size_t)]),
+        "XAMG_b200_mlp_destroy": (C.c_int, [C.c_size_t]),
+        "XAMG_b200_mlp_predict": (C.c_int, [C.c_size_t, C.c_uint32, vp, vp]),
+        "XAMG_b200_mlp_train_step": (C.c_int, [C.c_size_t, C.c_uint32, vp, vp, C.c_float,
+                                               C.POINTER(C.c_double)]),
+        "XAMG_b200_mlp_gradients": (C.c_int, [C.c_size_t, C.c_uint32, vp, vp, vp,
+                                              C.POINTER(C.c_double)]),
+        "XAMG_b200_mlp_params": (C.c_int, [C.c_size_t, vp, C.c_int, C.POINTER(u64)]),
         "XAMG_b200_matrix_hierarchy_load": (C.c_int, [C.c_size_t, C.c_char_p]),
     }
     for name, (res, args) in sig.items():
@@ -359,6 +370,50 @@ class Matrix:
         """Attach a hierarchy file written for this matrix (skips the setup of
         solvers created with the same multigrid parameters)."""
         call("XAMG_b200_matrix_hierarchy_load", self.h, str(path).encode())
+
+
+class Mlp:
+    """The learned-guess MLP (XAMG_b200_mlp_*): n_in -> h -> h -> n_out."""
+
+    def __init__(self, n_in, n_hidden, n_out, seed=0):
+        i = C.c_size_t()
+        call("XAMG_b200_mlp_create", n_in, n_hidden, n_out, seed, C.byref(i))
+        self.h, self.n_in, self.n_hidden, self.n_out = i.value, n_in, n_hidden, n_out
+
+    def __del__(self):
+        try:
+            call("XAMG_b200_mlp_destroy", self.h)
+        except Exception:
+            pass
+
+    def count(self):
+        c = u64()
+        call("XAMG_b200_mlp_params", self.h, None, 0, C.byref(c))
+        return c.value
+
+    def params(self):
+        out = np.zeros(self.count(), np.float32)
+        call("XAMG_b200_mlp_params", self.h, _ptr(out), 0, None)
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.count()
+        call("XAMG_b200_mlp_params", self.h, _ptr(p), 1, None)
+
+    def predict(self, X_ptr, Y_ptr, batch):
+        call("XAMG_b200_mlp_predict", self.h, batch, X_ptr, Y_ptr)
+
+    def train_step(self, X_ptr, T_ptr, batch, lr):
+        loss = C.c_double()
+        call("XAMG_b200_mlp_train_step", self.h, batch, X_ptr, T_ptr, lr, C.byref(loss))
+        return loss.value
+
+    def gradients(self, X_ptr, T_ptr, batch):
+        g = np.zeros(self.count(), np.float32)
+        loss = C.c_double()
+        call("XAMG_b200_mlp_gradients", self.h, batch, X_ptr, T_ptr, _ptr(g), C.byref(loss))
+        return g, loss.value
 
 
 class Vector:
