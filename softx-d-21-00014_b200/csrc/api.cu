@@ -350,7 +350,7 @@ int XAMG_vector_upload_d(double *ptr, uint64_t block_size, uint64_t block_offset
         XG_REQUIRE(ptr || block_size == 0, XAMG_ERR_INVALID_ARG, "null host pointer");
         if (block_size)
             XG_CUDA(cudaMemcpyAsync(v.v.p<double>() + block_offset * nv, ptr,
-                                    block_size * nv * sizeof(double), cudaMemcpyHostToDevice,
+                                    block_size * nv * sizeof(double), cudaMemcpyDefault,
                                     ctx().stream));
         XG_CUDA(cudaStreamSynchronize(ctx().stream));
         v.v.zero = false;
@@ -366,11 +366,17 @@ int XAMG_vector_download_d(double *ptr, uint64_t block_size, uint64_t block_offs
         XG_REQUIRE(block_offset + block_size <= v.v.n, XAMG_ERR_INVALID_ARG,
                    "block exceeds the vector");
         if (block_size) {
-            if (v.v.zero) {
+            cudaPointerAttributes pa;
+            const bool on_device = cudaPointerGetAttributes(&pa, ptr) == cudaSuccess &&
+                                   pa.type == cudaMemoryTypeDevice;
+            cudaGetLastError();
+            if (v.v.zero && on_device) {
+                XG_CUDA(cudaMemsetAsync(ptr, 0, block_size * nv * sizeof(double), ctx().stream));
+            } else if (v.v.zero) {
                 std::memset(ptr, 0, block_size * nv * sizeof(double));
             } else {
                 XG_CUDA(cudaMemcpyAsync(ptr, v.v.p<double>() + block_offset * nv,
-                                        block_size * nv * sizeof(double), cudaMemcpyDeviceToHost,
+                                        block_size * nv * sizeof(double), cudaMemcpyDefault,
                                         ctx().stream));
             }
         }
