@@ -5,7 +5,7 @@
 // the only tensor-core work of the solve phase.
 //
 // One CTA computes a 128 x 128 tile: warp 0 streams 128 x 64 tiles of A and B
-// into a four-stage ring of 128-byte-swizzled shared-memory buffers with TMA
+// into a ring of 128-byte-swizzled shared-memory stages with TMA
 // (cp.async.bulk.tensor, completion on an mbarrier per stage), warp 1 issues
 // tcgen05.mma (M = 128, N = 128, K = 16 per instruction) into a 128-column
 // TMEM accumulator and releases each stage with tcgen05.commit, and warps 2-5
@@ -24,7 +24,13 @@ namespace xg {
 namespace ops {
 namespace mm {
 
-constexpr int BM = 128, BN = 128, BK = 64, STAGES = 4;
+#ifndef XG_GEMM_STAGES
+#define XG_GEMM_STAGES 3
+#endif
+// Three stages (97 KB of shared memory) let two CTAs share an SM, so that one
+// CTA's epilogue overlaps the other's main loop.
+constexpr int BM = 128, BN = 128, BK = 64, STAGES = XG_GEMM_STAGES;
+constexpr int CTAS_PER_SM = STAGES <= 3 ? 2 : 1;
 constexpr uint32_t TILE_A = BM * BK * 2, TILE_B = BN * BK * 2;  // 16 KB each
 constexpr uint32_t STAGE_BYTES = TILE_A + TILE_B;
 constexpr uint32_t SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + alignment slack
@@ -110,7 +116,7 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__global__ void __launch_bounds__(THREADS, 1)
+__global__ void __launch_bounds__(THREADS, CTAS_PER_SM)
     k_gemm_bf16(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb,
                 int K, void *C, uint64_t ldc, int mode, const float *__restrict__ bias,
                 const __nv_bfloat16 *__restrict__ aux, uint64_t ld_aux, unsigned *flag) {
