@@ -40,6 +40,10 @@ WORKLOADS = {
                   order=2),
     "poisson32": dict(desc="7-pt Poisson 32^3 (cube.inl), nv=1, MergedPBiCGStab + Jacobi",
                       stencil=0, grid=32, sigma=0.0, aniso=1.0, nv=1, smoother=None, order=0),
+    "aniso192": dict(desc="27-pt var-kappa Q1 FE 192^3, kappa=exp(N(0,4)), 4:1 z-anisotropy, nv=32, "
+                          "PBiCGStab + AMG V(2,2) Chebyshev-3",
+                     stencil=27, grid=192, sigma=2.0, aniso=4.0, nv=32, smoother="Chebyshev",
+                     order=3, sweeps=2),
     "learned96": dict(desc="7-pt var-kappa 96^3, nv=32, learned coarse guess vs zero guess "
                            "(4096 training, 1024 held-out Gaussian-source RHS)",
                       stencil=7, grid=96, sigma=1.0, aniso=1.0, nv=32, smoother="Chebyshev",
@@ -53,6 +57,8 @@ def params_for(w, reduced):
                            "rel_tolerance": 1e-8, "abs_tolerance": 0},
                 "preconditioner": {"method": "Jacobi"}}
     sm = {"method": w["smoother"], "polynomial_order": w["order"]}
+    if w.get("sweeps", 1) != 1:
+        sm["max_iters"] = w["sweeps"]
     # plain: XAMG's FP64 method with XAMG's index narrowing. chosen: the whole
     # multigrid preconditioner (finest level included) in FP32 with 2-byte
     # column offsets where they fit; the outer iteration stays FP64.
