@@ -454,17 +454,19 @@ __global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
         const uint64_t r0 = tile * R;
         const uint64_t r1 = r0 + R < n ? r0 + R : n;
         const uint32_t tj0 = __ldg(&row[r0]), tj1 = __ldg(&row[r1]);
-        const bool staged = tj1 - tj0 <= CAP;
+        bool staged = tj1 - tj0 <= CAP;
         if (nbuf == 2 && threadIdx.x == 0) issue(tnext);
         const F *sv = nullptr;
         const I *sc = nullptr;
         if (staged) {
             const uint32_t b = n_used % nbuf;
+            // a copy that never landed: raise the flag, read global memory
             if (!mbar_wait(&mbar[b], (n_used / nbuf) & 1u)) timed_out = true;
             ++n_used;
             const unsigned char *buf = smem_raw + (size_t)b * BB;
             sv = (const F *)buf + stage_shift<F>(val, tj0);
             sc = (const I *)(buf + VB) + stage_shift<I>(col, tj0);
+            staged = !timed_out;
         }
         const uint64_t i = r0 + rt;
         if (i < n) {

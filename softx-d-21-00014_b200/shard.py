@@ -102,13 +102,15 @@ class LibraryCompute:
         self.X, self.torch, self.keep = X, torch, {}
 
     def _desc(self, blk, ncols):
+        # keyed by the block's identity; the entry keeps the block alive so
+        # that its id is not reused by another block
         key = id(blk)
         if key not in self.keep:
             t = self.torch
             r, c, v = (t.from_numpy(a).cuda() for a in blk)
             d = self.X.Csr(len(blk[0]) - 1, ncols, len(blk[1]), r.data_ptr(), c.data_ptr(),
                            v.data_ptr(), 4, 0)
-            self.keep[key] = (d, r, c, v)
+            self.keep[key] = (d, r, c, v, blk)
         return self.keep[key][0]
 
     def ax_y(self, blk, x, nrows, nv):

@@ -1,19 +1,20 @@
 """The SpMV on a solver's own level matrices (XAMG_b200_solver_level_spmv),
 as its solves run it: the library's uploaded copy with XAMG's narrowing or
 2-byte relative columns, FP64 on the Krylov level and FP32 on the cycle's
-level 0 with gpu_precond_f32. Every element must equal the oracle's
-sequential row sum bit for bit, for y = A x and y += A x. The matrices mix
-banded rows with rows of far-off random columns, with row counts that leave
-ragged last tiles."""
+level 0 with gpu_precond_f32. Every element must equal
+the oracle's sequential row sum bit for bit, for y = A x and y += A x. The
+matrices mix banded rows with rows of far-off random columns, with row counts
+that leave ragged last tiles, and rows stored sorted or diagonal first."""
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
 
-def banded_plus_random(n, far_from, n_far, seed):
+def banded_plus_random(n, far_from, n_far, seed, diag_first=False):
     """7-point band of a 3-D grid of n rows (plus-minus 1, nx, nx*ny), and
-    from row far_from on n_far extra random columns per row."""
+    from row far_from on n_far extra random columns per row; diag_first
+    stores each row's diagonal first, as hypre does."""
     rng = np.random.default_rng(seed)
     nx, ny = 13, 11
     row, cols, vals = [0], [], []
@@ -27,6 +28,8 @@ def banded_plus_random(n, far_from, n_far, seed):
         if i >= far_from:
             c.update(int(v) for v in rng.integers(0, n, n_far))
         c = sorted(c)
+        if diag_first:
+            c = [i] + [v for v in c if v != i]
         cols.extend(c)
         vals.extend((rng.standard_normal(len(c)) + np.where(np.array(c) == i, 8.0, 0.0)).tolist())
         row.append(len(cols))
@@ -57,15 +60,17 @@ def run_level_spmv(gpu, S, level, which, row, col, val, nv, f32, seed):
     return xh, y0, y.cpu().numpy(), ya.cpu().numpy()
 
 
-KRYLOV = {"solver": {"method": "MergedPBiCGStab", "rel_tolerance": 1e-8, "max_iters": 10},
-          "preconditioner": {"method": "Jacobi"}}
+def krylov():
+    return {"solver": {"method": "MergedPBiCGStab", "rel_tolerance": 1e-8, "max_iters": 10},
+            "preconditioner": {"method": "Jacobi"}}
 
 
-@pytest.mark.parametrize("nv", [2, 4, 8, 16, 32])
-@pytest.mark.parametrize("n,far_from", [(3001, 2400), (2000, 2000), (257, 200)])
-def test_fp64_level_spmv_bit_exact(gpu, oracle, nv, n, far_from):
-    row, col, val = banded_plus_random(n, far_from, 9, seed=n + nv)
-    _, _, _, S = solver_on(gpu, row, col, val, nv, KRYLOV)
+@pytest.mark.parametrize("nv", [1, 2, 4, 8, 16, 32])
+@pytest.mark.parametrize("n,far_from,diag_first", [(3001, 2400, False), (2000, 2000, True),
+                                                   (257, 200, False), (1003, 1003, True)])
+def test_fp64_level_spmv_bit_exact(gpu, oracle, nv, n, far_from, diag_first):
+    row, col, val = banded_plus_random(n, far_from, 9, seed=n + nv, diag_first=diag_first)
+    _, _, _, S = solver_on(gpu, row, col, val, nv, krylov())
     xh, y0, y, ya = run_level_spmv(gpu, S, 0, 0, row, col, val, nv, False, seed=nv)
     want = oracle.csr_ax_y(row, col, val, xh, nv)
     assert y.tobytes() == want.tobytes()
@@ -73,7 +78,7 @@ def test_fp64_level_spmv_bit_exact(gpu, oracle, nv, n, far_from):
     assert ya.tobytes() == want_a.tobytes()
 
 
-@pytest.mark.parametrize("nv", [4, 8, 32])
+@pytest.mark.parametrize("nv", [1, 4, 8, 32])
 def test_fp32_cycle_operator_bit_exact(gpu, oracle, nv):
     """Level 0 of an FP32 multigrid preconditioner (gpu_precond_f32 = 1),
     with 2-byte relative columns, on a 27-point FE matrix."""
@@ -90,3 +95,19 @@ def test_fp32_cycle_operator_bit_exact(gpu, oracle, nv):
     v32 = val.astype(np.float32)
     assert y.tobytes() == oracle.csr_ax_y(row, col, v32, xh, nv).tobytes()
     assert ya.tobytes() == oracle.csr_ax_y(row, col, v32, xh, nv, axpy_y=y0).tobytes()
+
+
+@pytest.mark.parametrize("nv", [1, 8, 32])
+def test_fp64_27pt_diag_first(gpu, oracle, nv):
+    """27-point FE rows stored diagonal first (hypre's order)."""
+    row, col, val = gpu.generate_diffusion(27, 13, 12, 11, 1.0, 1.0, 5)
+    col, val = col.copy(), val.copy()
+    for i in range(len(row) - 1):
+        a, b = int(row[i]), int(row[i + 1])
+        d = a + int(np.nonzero(col[a:b] == i)[0][0])
+        order = [d] + [j for j in range(a, b) if j != d]
+        col[a:b], val[a:b] = col[order], val[order]
+    _, _, _, S = solver_on(gpu, row, col, val, nv, krylov())
+    xh, y0, y, ya = run_level_spmv(gpu, S, 0, 0, row, col, val, nv, False, seed=nv)
+    assert y.tobytes() == oracle.csr_ax_y(row, col, val, xh, nv).tobytes()
+    assert ya.tobytes() == oracle.csr_ax_y(row, col, val, xh, nv, axpy_y=y0).tobytes()
