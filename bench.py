@@ -44,6 +44,11 @@ WORKLOADS = {
                           "PBiCGStab + AMG V(2,2) Chebyshev-3",
                      stencil=27, grid=192, sigma=2.0, aniso=4.0, nv=32, smoother="Chebyshev",
                      order=3, sweeps=2),
+    "batch64": dict(desc="64 uneven 7-pt var-kappa systems, edge in {16,24,...,96}, "
+                         "kappa=exp(N(0,1.5^2)), nv in {1,4,16}, PBiCGStab + AMG V(1,1) HSGS "
+                         "FP32, batch solve vs one solve per call",
+                    stencil=7, grid=96, sigma=1.5, aniso=1.0, nv=0, smoother="HSGS", order=0,
+                    systems=64),
     "learned96": dict(desc="7-pt var-kappa 96^3, nv=32, learned coarse guess vs zero guess "
                            "(4096 training, 1024 held-out Gaussian-source RHS)",
                       stencil=7, grid=96, sigma=1.0, aniso=1.0, nv=32, smoother="Chebyshev",
@@ -398,6 +403,132 @@ def run_reference(args, w):
                     "d2h_bytes_per_step": 0}}
 
 
+def batch_params(reduced):
+    """Configuration 3's method: merged PBiCGStab with an AMG V(1,1)
+    hybrid-Gauss-Seidel preconditioner, FP32 with 2-byte relative columns
+    (chosen) or XAMG's FP64 method (plain)."""
+    sm = {"method": "HSGS", "max_iters": 1}
+    prec = {"method": "MultiGrid", "max_iters": 1, "mg_agg_num_levels": 0,
+            "mg_strength_threshold": 0.25, "mg_coarsening_type": 8,
+            "mg_interpolation_type": 6, "mg_coarse_matrix_size": 500,
+            "mg_reduced_precision": 0, "gpu_index_compress": 1}
+    solver = {"method": "MergedPBiCGStab", "max_iters": 500, "rel_tolerance": 1e-8,
+              "abs_tolerance": 0, "gpu_index_compress": 1}
+    if reduced:
+        prec.update(gpu_precond_f32=1, gpu_index_compress=2)
+        solver.update(gpu_index_compress=2)
+    return {"solver": solver, "preconditioner": prec, "pre_smoother": sm,
+            "post_smoother": dict(sm), "coarse_grid_solver": {"method": "Direct"}}
+
+
+def run_batch(args, w):
+    """Configuration 3: the systems solved by one XAMG_b200_solver_solve_batch
+    call per step (chosen: FP32 preconditioner, every system on its own
+    stream, lockstep iterations) against one XAMG_solver_solve2 call per
+    system (the same solvers, and XAMG's plain FP64 method). Synthetic
+    systems: edges and nv drawn from a seeded generator."""
+    import torch
+    import xamg_b200 as X
+    X.init()
+    stream = torch.cuda.ExternalStream(X.stream())
+    rng = np.random.default_rng(3)
+    m = w["systems"]
+    edges = rng.choice(np.arange(16, 97, 8), m)
+    nvs = rng.choice([1, 4, 16], m)
+    t0 = time.time()
+    sysm = []
+    for i in range(m):
+        e, nv = int(edges[i]), int(nvs[i])
+        row, col, val = X.generate_diffusion(7, e, e, e, w["sigma"], 1.0, 100 + i)
+        n = len(row) - 1
+        M = X.Matrix(row, col, val)
+        b = rng.uniform(-1, 1, n * nv)
+        bv, xv = X.Vector(n, nv), X.Vector(n, nv)
+        bv.upload(b)
+        xv.set(0.0)
+        S = X.Solver(M, X.Params(batch_params(True)), xv, bv)
+        P = X.Solver(M, X.Params(batch_params(False)), xv, bv)
+        sysm.append(dict(M=M, b=b, bv=bv, xv=xv, S=S, P=P, n=n, nv=nv,
+                         bh=torch.from_numpy(b).pin_memory(),
+                         xh=torch.empty(n * nv, dtype=torch.float64).pin_memory(),
+                         row=row, col=col, val=val))
+    setup_s = time.time() - t0
+    total_rhs = int(nvs.sum())
+    Ss = [d["S"] for d in sysm]
+    xs = [d["xv"] for d in sysm]
+    bs = [d["bv"] for d in sysm]
+
+    def step(kind, e2e=False):
+        if e2e:
+            for d in sysm:
+                X.call("XAMG_vector_upload_d", d["bh"].data_ptr(), d["n"], 0, d["nv"], d["bv"].h)
+        for d in sysm:
+            d["xv"].set(0.0)
+        if kind == "batch":
+            X.solve_batch(Ss, xs, bs)
+        else:
+            for d in sysm:
+                (d["S"] if kind == "single" else d["P"]).solve(d["xv"], d["bv"])
+        if e2e:
+            for d in sysm:
+                X.call("XAMG_vector_download_d", d["xh"].data_ptr(), d["n"], 0, d["nv"],
+                       d["xv"].h)
+
+    def timed(kind, K, e2e=False):
+        for _ in range(args.warmup):
+            step(kind)
+        torch.cuda.synchronize()
+        k0 = X.kernel_launches()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for _ in range(K):
+                step(kind, e2e)
+            e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / K, (X.kernel_launches() - k0) // K
+
+    with ClockSampler(0) as cs:
+        ms_batch, launches = timed("batch", args.steps)
+    ms_single, _ = timed("single", args.steps)
+    ms_plain, _ = timed("plain", max(1, args.steps // 2))
+    ms_e2e, _ = timed("batch", args.steps, e2e=True)
+    iters = [int(np.max(d["S"].stats()["iters"])) for d in sysm]
+    # true residuals of the batch solve (from the last e2e step's downloads)
+    import scipy.sparse as sp
+    worst = 0.0
+    for d in sysm:
+        A = sp.csr_matrix((d["val"].copy(), d["col"].copy(), d["row"].copy()),
+                          shape=(d["n"], d["n"]))
+        Xs, Bs = d["xh"].numpy().reshape(d["n"], d["nv"]), d["b"].reshape(d["n"], d["nv"])
+        worst = max(worst, float((np.linalg.norm(Bs - A @ Xs, axis=0) /
+                                  np.linalg.norm(Bs, axis=0)).max()))
+    big = int(np.argmax([d["n"] * d["nv"] for d in sysm]))
+    rf = roofline(X, torch, stream, sysm[big]["S"], sysm[big]["n"], sysm[big]["nv"], args)
+    rf["kernel"] += f" (largest system: {int(edges[big])}^3, nv={int(nvs[big])})"
+    return {
+        "metric": "ms/RHS to 1e-8 residual: batch solve vs one solve per call on 1 B200",
+        "value": ms_batch / total_rhs, "unit": "ms/RHS", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_batch, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 outer / f32 preconditioner",
+        "data": "synthetic",
+        "config": {"workload": w["desc"], "systems": m, "rows": int(sum(d["n"] for d in sysm)),
+                   "rhs_per_step": total_rhs, "edges": edges.tolist(), "nv": nvs.tolist(),
+                   "tolerance": 1e-8, "l2": "inputs larger than L2 (all systems' matrices)"},
+        "iters": {"min": min(iters), "max": max(iters), "mean": float(np.mean(iters))},
+        "one_call_per_system_ms_per_rhs": ms_single / total_rhs,
+        "plain_fp64_ms_per_rhs": ms_plain / total_rhs,
+        "batch_vs_one_call_speedup": ms_single / ms_batch,
+        "chosen_vs_fp64_speedup": ms_plain / ms_batch,
+        "true_rel_residual": worst,
+        "e2e": {"value": ms_e2e / total_rhs, "unit": "ms/RHS",
+                "h2d_bytes_per_step": int(sum(d["n"] * d["nv"] * 8 for d in sysm)),
+                "d2h_bytes_per_step": int(sum(d["n"] * d["nv"] * 8 for d in sysm))},
+        "gpu_launches": int(launches), "roofline": rf, "clocks": cs.summary(),
+        "setup_s": setup_s,
+    }
+
+
 def run_learned(args, w):
     """The learned coarse initial guess (configuration 4): not the headline
     metric; one JSON line with both guesses' iterations and ms/RHS."""
@@ -432,6 +563,8 @@ def main():
         w["desc"] = w["desc"].replace("128^3", f"{args.grid}^3").replace("32^3", f"{args.grid}^3")
     if args.workload == "learned96" and args.impl != "reference":
         out = run_learned(args, w)
+    elif args.workload == "batch64" and args.impl != "reference":
+        out = run_batch(args, w)
     else:
         out = run_reference(args, w) if args.impl == "reference" else run_ours(args, w)
     if out is not None:

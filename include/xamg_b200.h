@@ -235,6 +235,17 @@ int XAMG_b200_vector_device_ptr(size_t vid, void **ptr);
  * the solve call. */
 int XAMG_b200_wait_selftest(double seconds, int *timed_out);
 
+/* Solves `count` independent systems together: entry i is
+ * XAMG_solver_solve2(nv[i], xids[i], bids[i], sids[i]) (xamg_c_api.h:112),
+ * with the same results bit for bit, but every system runs on a stream and
+ * reduction scratch of its own so that their kernels run concurrently, and
+ * the merged BiCGStab forms advance in lockstep with one host
+ * synchronisation per iteration for the whole batch (no counterpart in the
+ * reference, which solves one system per call). Solvers and solution vectors
+ * must be distinct; the call returns when every system is finished. */
+int XAMG_b200_solver_solve_batch(int count, const uint16_t *nv, const size_t *xids,
+                                 const size_t *bids, const size_t *sids);
+
 #ifdef __cplusplus
 }
 #endif

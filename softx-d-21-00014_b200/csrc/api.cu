@@ -7,6 +7,7 @@
 
 #include <cstring>
 #include <map>
+#include <set>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -618,6 +619,38 @@ int XAMG_solver_solve2(uint16_t nv, XAMG_vector_id xid, XAMG_vector_id bid, XAMG
     return guarded([&] {
         SolverObj &so = get(g_solvers, sid, "solver");
         do_solve(so, get(g_vecs, xid, "vector"), get(g_vecs, bid, "vector"), nv);
+    });
+}
+
+int XAMG_b200_solver_solve_batch(int count, const uint16_t *nv, const XAMG_vector_id *xids,
+                                 const XAMG_vector_id *bids, const XAMG_solver_id *sids) {
+    return guarded([&] {
+        XG_REQUIRE(count >= 0 && count <= 4095, XAMG_ERR_INVALID_ARG,
+                   "batch size must be in [0, 4095]");
+        if (count == 0) return;
+        XG_REQUIRE(nv && xids && bids && sids, XAMG_ERR_INVALID_ARG, "null array");
+        std::vector<SolverHierarchy *> hs;
+        std::vector<DVec *> xs, bs;
+        std::set<size_t> seen_s, seen_x;
+        for (int i = 0; i < count; ++i) {
+            SolverObj &so = get(g_solvers, sids[i], "solver");
+            VecObj &x = get(g_vecs, xids[i], "vector");
+            VecObj &b = get(g_vecs, bids[i], "vector");
+            XG_REQUIRE(seen_s.insert(sids[i]).second && seen_x.insert(xids[i]).second,
+                       XAMG_ERR_INVALID_ARG, "a solver or solution vector appears twice");
+            check_nv(nv[i]);
+            XG_REQUIRE(x.allocated && b.allocated, XAMG_ERR_INVALID_ARG, "vector not allocated");
+            XG_REQUIRE(x.v.nv == nv[i] && b.v.nv == nv[i], XAMG_ERR_NV_MISMATCH,
+                       "nv differs from the vectors' nv");
+            MatObj &m = get(g_mats, so.mid, "matrix");
+            XG_REQUIRE(x.v.n == m.h.nrows && b.v.n == m.h.nrows, XAMG_ERR_INVALID_ARG,
+                       "vector size differs from the matrix size");
+            if (nv[i] != so.nv) build_solver(so, so.sh->params, nv[i]);
+            hs.push_back(so.sh.get());
+            xs.push_back(&x.v);
+            bs.push_back(&b.v);
+        }
+        solve_batch(hs, xs, bs);
     });
 }
 

@@ -57,8 +57,19 @@ struct DevBuf {
     }
 };
 
+// A stream with its own reduction scratch and pinned host slots: the state a
+// solve's kernels and scalar read-backs use. Lane 0 is the library's stream;
+// the batch solve runs each system on a lane of its own, so that their
+// kernels run concurrently without sharing scratch.
+struct Lane {
+    cudaStream_t stream = nullptr;
+    DevBuf red_part, red_ticket, red_out;
+    double *pinned = nullptr;
+};
+
 // Process-wide state created by XAMG_init (or lazily by the first call that
-// needs the GPU).
+// needs the GPU). The stream and scratch fields are those of the current
+// lane (use_lane swaps them).
 struct Ctx {
     cudaStream_t stream = nullptr;
     DevBuf red_part;    // canonical-reduction partials: BMAX x 32 x 3 doubles
@@ -70,9 +81,13 @@ struct Ctx {
     int sms = 148;            // streaming multiprocessors of the device
     int device_request = -1;  // set by XAMG_b200_set_device before init
     bool ready = false;
+    int lane = 0;             // current lane
+    std::vector<Lane> lanes;  // parked state of the lanes not current
 
     void init();
     void shutdown();
+    // Makes lane i current (creating it on first use); lane 0 is the default.
+    void use_lane(int i);
     k::RedArgs red() const {
         return k::RedArgs{red_part.p, red_ticket.as<unsigned>(), red_ticket.as<unsigned>() + 2};
     }

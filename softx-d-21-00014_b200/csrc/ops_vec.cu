@@ -17,6 +17,38 @@ Ctx &ctx() {
 
 Ctx &ctx_uninit() { return g_ctx; }
 
+// Creates a lane's stream, scratch and pinned slots (the fields of Ctx or of
+// a parked Lane).
+static void lane_create(cudaStream_t &stream, DevBuf &part, DevBuf &ticket, DevBuf &out,
+                        double *&pinned) {
+    XG_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    part.alloc((size_t)k::BMAX * 32 * 4 * sizeof(double));
+    ticket.alloc(sizeof(unsigned) * 4);
+    out.alloc(128 * sizeof(double));
+    XG_CUDA(cudaMemsetAsync(ticket.p, 0, ticket.bytes, stream));
+    XG_CUDA(cudaMallocHost((void **)&pinned, 256 * sizeof(double)));
+    XG_CUDA(cudaStreamSynchronize(stream));
+}
+
+static void lane_swap(Ctx &c, Lane &l) {
+    std::swap(c.stream, l.stream);
+    std::swap(c.red_part, l.red_part);
+    std::swap(c.red_ticket, l.red_ticket);
+    std::swap(c.red_out, l.red_out);
+    std::swap(c.pinned, l.pinned);
+}
+
+void Ctx::use_lane(int i) {
+    XG_REQUIRE(i >= 0 && i <= 4096, XAMG_ERR_INVALID_ARG, "lane out of range");
+    if (i == lane) return;
+    if ((int)lanes.size() <= std::max(i, lane)) lanes.resize(std::max(i, lane) + 1);
+    Lane &l = lanes[i];
+    if (!l.stream) lane_create(l.stream, l.red_part, l.red_ticket, l.red_out, l.pinned);
+    lane_swap(*this, lanes[lane]);  // park the current lane
+    lane_swap(*this, lanes[i]);     // take lane i
+    lane = i;
+}
+
 void Ctx::init() {
     if (ready) return;
     int ndev = 0;
@@ -27,13 +59,8 @@ void Ctx::init() {
     if (device_request >= 0) XG_CUDA(cudaSetDevice(device_request));
     XG_CUDA(cudaGetDevice(&device));
     XG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    XG_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-    red_part.alloc((size_t)k::BMAX * 32 * 4 * sizeof(double));
-    red_ticket.alloc(sizeof(unsigned) * 4);
-    red_out.alloc(128 * sizeof(double));
-    XG_CUDA(cudaMemsetAsync(red_ticket.p, 0, red_ticket.bytes, stream));
-    XG_CUDA(cudaMallocHost((void **)&pinned, 256 * sizeof(double)));
-    XG_CUDA(cudaStreamSynchronize(stream));
+    lane_create(stream, red_part, red_ticket, red_out, pinned);
+    lane = 0;
     ready = true;
 }
 
@@ -51,6 +78,19 @@ void Ctx::check_flags() {
 
 void Ctx::shutdown() {
     if (!ready) return;
+    use_lane(0);
+    for (Lane &l : lanes) {
+        if (!l.stream) continue;
+        cudaStreamSynchronize(l.stream);
+        l.red_part.release();
+        l.red_ticket.release();
+        l.red_out.release();
+        if (l.pinned) cudaFreeHost(l.pinned);
+        l.pinned = nullptr;
+        cudaStreamDestroy(l.stream);
+        l.stream = nullptr;
+    }
+    lanes.clear();
     cudaStreamSynchronize(stream);
     red_part.release();
     red_ticket.release();

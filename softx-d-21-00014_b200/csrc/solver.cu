@@ -184,6 +184,7 @@ struct Jacobi : public SolverBase {
 template <typename F>
 struct Hsgs : public SolverBase {
     DevBuf d, boff, relax_dev;
+    std::vector<double> relax_on_dev;  // what relax_dev holds (host mirror)
     DCsr Adiag, Aoff;
     int nblocks = 1;
     void setup_from(const HCsr &hA) {
@@ -237,8 +238,9 @@ struct Hsgs : public SolverBase {
         else
             upload(d, inv_diag_f64(hA, false), S());
         relax_dev.alloc(32 * sizeof(double));
-        std::vector<double> rh(32, (double)(F)cfg.relax);
-        XG_CUDA(cudaMemcpy(relax_dev.p, rh.data(), 32 * sizeof(double), cudaMemcpyHostToDevice));
+        relax_on_dev.assign(32, (double)(F)cfg.relax);
+        XG_CUDA(cudaMemcpyAsync(relax_dev.p, relax_on_dev.data(), 32 * sizeof(double),
+                                cudaMemcpyHostToDevice, S()));
         alloc_buffers(2);
         XG_CUDA(cudaStreamSynchronize(S()));
     }
@@ -256,10 +258,15 @@ struct Hsgs : public SolverBase {
         }
         do {
             ++st.iters;
-            // scal(iconv, relax_conv) (hsgs.inl:102)
-            if (!ones || cfg.convergence_check) {
+            // scal(iconv, relax_conv) (hsgs.inl:102); the device copy is
+            // refreshed whenever it differs, so a solve that starts with every
+            // right-hand side active does not inherit the factors an earlier
+            // solve froze
+            if (!ones || cfg.convergence_check)
                 for (int k = 0; k < NV; ++k) relax_h[k] = (double)(F)(relax_h[k] * iconv[k]);
-                XG_CUDA(cudaMemcpyAsync(relax_dev.p, relax_h.data(), NV * sizeof(double),
+            if (!std::equal(relax_h.begin(), relax_h.end(), relax_on_dev.begin())) {
+                std::copy(relax_h.begin(), relax_h.end(), relax_on_dev.begin());
+                XG_CUDA(cudaMemcpyAsync(relax_dev.p, relax_on_dev.data(), NV * sizeof(double),
                                         cudaMemcpyHostToDevice, S()));
             }
             if (x.zero) {
@@ -689,7 +696,8 @@ void Krylov::apply_M(DVec &out, DVec &in) {
         run_M(out, in);
         return;
     }
-    MGraph &g = graphs_[std::make_tuple(out.p<const void>(), in.p<const void>(), in.zero)];
+    MGraph &g =
+        graphs_[std::make_tuple(out.p<const void>(), in.p<const void>(), in.zero, ctx().lane)];
     if (g.exec) {
         XG_CUDA(cudaGraphLaunch(g.exec, S()));
         g_kernel_launches += g.launches;
@@ -840,17 +848,42 @@ void Krylov::solve(DVec &x, DVec &b, const std::vector<double> &conv) {
         solve_rbicgstab(x, b, conv);
         return;
     }
+    begin(x, b, conv);
+    XG_CUDA(cudaStreamSynchronize(S()));
+    if (started()) return;
+    while (true) {
+        step();
+        XG_CUDA(cudaStreamSynchronize(S()));
+        if (stepped()) return;
+        if (st.iters >= cfg.max_iters) break;
+    }
+    XG_CUDA(cudaStreamSynchronize(S()));
+}
+
+// Posts nv device scalars to the current lane's pinned slots; take_scalars
+// reads them once the lane's stream has been synchronised.
+static void post_scalars(const double *dev, int nv) {
+    Ctx &c = ctx();
+    XG_CUDA(cudaMemcpyAsync(c.pinned, dev, nv * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+}
+static void take_scalars(double *host, int nv) { std::memcpy(host, ctx().pinned, nv * sizeof(double)); }
+
+// merged_bicgstab.inl:44-208 / merged_pbicgstab.inl:44-225
+void Krylov::begin(DVec &x, DVec &b, const std::vector<double> &conv) {
+    reset_stats();
     cudaStream_t s = S();
-    std::vector<double> iconv = conv;
-    upload_iconv(iconv);
+    run_.x = &x;
+    run_.b = &b;
+    run_.iconv = conv;
+    run_.rho0.assign(NV, 0.0);
+    run_.res.assign(NV, 0.0);
+    upload_iconv(run_.iconv);
     double *SC = sc.as<double>();
     for (auto &v : buf) {
         v.zero = true;
         v.init = true;
     }
-    DVec &r0 = buf[0], &r = buf[1], &p = buf[2], &v = buf[3], &s_ = buf[4], &t = buf[5],
-         &p_ = buf[6], &s2 = buf[7];
-    std::vector<double> rho0(NV), res(NV);
+    DVec &r0 = buf[0], &r = buf[1], &p = buf[2];
     // 1-2: r0 = b - A x; rho0 = (r0, r0); p = r = r0 (rho = rho0)
     if (x.zero)
         ops::group1_zero(n, b.p<double>(), r0.p<double>(), p.p<double>(), r.p<double>(), SC, NV, s);
@@ -858,56 +891,73 @@ void Krylov::solve(DVec &x, DVec &b, const std::vector<double> &conv) {
         ops::group1(*A, x.p<double>(), b.p<double>(), r0.p<double>(), p.p<double>(),
                     r.p<double>(), SC, NV, s);
     r0.zero = p.zero = r.zero = false;
-    read_scalars(SC + k::SC_RHO0 * k::SC_STRIDE, rho0.data(), NV);
-    if (check(rho0.data(), rho0.data(), iconv)) return;
-    const bool has_M = (M != nullptr);
-    do {
-        ++st.iters;
-        DVec *pa = &p, *sa = &s_;
-        if (has_M) {
-            apply_M(p_, p);
-            pa = &p_;
-        }
-        // v = A p_; alpha = rho / (v, r0)
-        ops::spmv_dot_alpha(*A, pa->p<double>(), v.p<double>(), r0.p<double>(), SC, NV, s);
-        v.zero = false;
-        // s = r - alpha v
-        ops::s_update(n, s_.p<double>(), r.p<double>(), v.p<double>(), SC, NV, s);
-        s_.zero = false;
-        if (has_M) {
-            apply_M(s2, s_);
-            sa = &s2;
-        }
-        // t = A s_; omega = (t,s)/(t,t); res = (s,s) - omega (t,s)
-        ops::spmv_dot3(*A, sa->p<double>(), t.p<double>(), s_.p<double>(), SC, NV, s);
-        t.zero = false;
-        read_scalars(SC + k::SC_RES * k::SC_STRIDE, res.data(), NV);
-        const bool done = check(res.data(), rho0.data(), iconv);
-        if (precond_form) {
-            if (done) {
-                ops::x_update(n, x.p<double>(), pa->p<double>(), sa->p<double>(), SC, NV, s);
-                x.zero = false;
-                return;
-            }
-            // x update fused with r = s - omega t; rho = (r, r0); beta
-            ops::group4(n, s_.p<double>(), t.p<double>(), r0.p<double>(), r.p<double>(),
-                        x.p<double>(), pa->p<double>(), sa->p<double>(), true, SC, NV, s);
+    post_scalars(SC + k::SC_RHO0 * k::SC_STRIDE, NV);
+}
+
+bool Krylov::started() {
+    take_scalars(run_.rho0.data(), NV);
+    return check(run_.rho0.data(), run_.rho0.data(), run_.iconv);
+}
+
+void Krylov::step() {
+    cudaStream_t s = S();
+    double *SC = sc.as<double>();
+    DVec &r0 = buf[0], &r = buf[1], &p = buf[2], &v = buf[3], &s_ = buf[4], &t = buf[5],
+         &p_ = buf[6], &s2 = buf[7];
+    ++st.iters;
+    run_.pa = &p;
+    run_.sa = &s_;
+    if (M) {
+        apply_M(p_, p);
+        run_.pa = &p_;
+    }
+    // v = A p_; alpha = rho / (v, r0)
+    ops::spmv_dot_alpha(*A, run_.pa->p<double>(), v.p<double>(), r0.p<double>(), SC, NV, s);
+    v.zero = false;
+    // s = r - alpha v
+    ops::s_update(n, s_.p<double>(), r.p<double>(), v.p<double>(), SC, NV, s);
+    s_.zero = false;
+    if (M) {
+        apply_M(s2, s_);
+        run_.sa = &s2;
+    }
+    // t = A s_; omega = (t,s)/(t,t); res = (s,s) - omega (t,s)
+    ops::spmv_dot3(*A, run_.sa->p<double>(), t.p<double>(), s_.p<double>(), SC, NV, s);
+    t.zero = false;
+    post_scalars(SC + k::SC_RES * k::SC_STRIDE, NV);
+}
+
+bool Krylov::stepped() {
+    cudaStream_t s = S();
+    double *SC = sc.as<double>();
+    DVec &r0 = buf[0], &r = buf[1], &p = buf[2], &v = buf[3], &s_ = buf[4], &t = buf[5];
+    DVec &x = *run_.x;
+    take_scalars(run_.res.data(), NV);
+    const bool done = check(run_.res.data(), run_.rho0.data(), run_.iconv);
+    if (precond_form) {
+        if (done) {
+            ops::x_update(n, x.p<double>(), run_.pa->p<double>(), run_.sa->p<double>(), SC, NV, s);
             x.zero = false;
-            ops::p_update(n, p.p<double>(), r.p<double>(), v.p<double>(), SC, NV, s);
-        } else {
-            if (done) {
-                ops::x_update(n, x.p<double>(), p.p<double>(), s_.p<double>(), SC, NV, s);
-                x.zero = false;
-                return;
-            }
-            ops::group4(n, s_.p<double>(), t.p<double>(), r0.p<double>(), r.p<double>(), nullptr,
-                        nullptr, nullptr, false, SC, NV, s);
-            ops::group5(n, x.p<double>(), p.p<double>(), s_.p<double>(), r.p<double>(),
-                        v.p<double>(), SC, NV, s);
-            x.zero = false;
+            return true;
         }
-    } while (st.iters < cfg.max_iters);
-    XG_CUDA(cudaStreamSynchronize(s));
+        // x update fused with r = s - omega t; rho = (r, r0); beta
+        ops::group4(n, s_.p<double>(), t.p<double>(), r0.p<double>(), r.p<double>(),
+                    x.p<double>(), run_.pa->p<double>(), run_.sa->p<double>(), true, SC, NV, s);
+        x.zero = false;
+        ops::p_update(n, p.p<double>(), r.p<double>(), v.p<double>(), SC, NV, s);
+    } else {
+        if (done) {
+            ops::x_update(n, x.p<double>(), p.p<double>(), s_.p<double>(), SC, NV, s);
+            x.zero = false;
+            return true;
+        }
+        ops::group4(n, s_.p<double>(), t.p<double>(), r0.p<double>(), r.p<double>(), nullptr,
+                    nullptr, nullptr, false, SC, NV, s);
+        ops::group5(n, x.p<double>(), p.p<double>(), s_.p<double>(), r.p<double>(),
+                    v.p<double>(), SC, NV, s);
+        x.zero = false;
+    }
+    return false;
 }
 
 // ===========================================================================
@@ -987,5 +1037,77 @@ void SolverHierarchy::solve(DVec &x, DVec &b) {
     root->solve(x, b, ones);
     XG_CUDA(cudaStreamSynchronize(ctx().stream));
 }
+
+void solve_batch(const std::vector<SolverHierarchy *> &hs, const std::vector<DVec *> &xs,
+                 const std::vector<DVec *> &bs) {
+    Ctx &c = ctx();
+    XG_REQUIRE(c.lane == 0, XAMG_ERR_INTERNAL, "batch solve started off lane 0");
+    const int m = (int)hs.size();
+    struct Guard {  // lane 0 current again on every exit; events released
+        cudaEvent_t ev = nullptr;
+        ~Guard() {
+            try {
+                ctx().use_lane(0);
+            } catch (...) {
+            }
+            if (ev) cudaEventDestroy(ev);
+        }
+    } guard;
+    XG_CUDA(cudaEventCreateWithFlags(&guard.ev, cudaEventDisableTiming));
+    XG_CUDA(cudaEventRecord(guard.ev, c.stream));
+    std::vector<Krylov *> kr(m, nullptr);
+    std::vector<char> live(m, 0);
+    for (int i = 0; i < m; ++i) {
+        c.use_lane(i + 1);
+        XG_CUDA(cudaStreamWaitEvent(c.stream, guard.ev, 0));
+    }
+    for (int i = 0; i < m; ++i) {
+        c.use_lane(i + 1);
+        std::vector<double> ones(hs[i]->NV, 1.0);
+        kr[i] = dynamic_cast<Krylov *>(hs[i]->root.get());
+        if (kr[i] && kr[i]->steppable()) {
+            kr[i]->begin(*xs[i], *bs[i], ones);
+            live[i] = 1;
+        } else {
+            hs[i]->root->solve(*xs[i], *bs[i], ones);
+        }
+    }
+    for (int i = 0; i < m; ++i)
+        if (live[i]) {
+            c.use_lane(i + 1);
+            XG_CUDA(cudaStreamSynchronize(c.stream));
+            if (kr[i]->started()) live[i] = 0;
+        }
+    for (;;) {
+        bool any = false;
+        for (int i = 0; i < m; ++i)
+            if (live[i]) {
+                c.use_lane(i + 1);
+                kr[i]->step();
+                any = true;
+            }
+        if (!any) break;
+        for (int i = 0; i < m; ++i)
+            if (live[i]) {
+                c.use_lane(i + 1);
+                XG_CUDA(cudaStreamSynchronize(c.stream));
+                if (kr[i]->stepped() || kr[i]->st.iters >= kr[i]->cfg.max_iters) live[i] = 0;
+            }
+    }
+    // join: lane 0 waits for every lane; then each lane's wait-timeout flag
+    for (int i = 0; i < m; ++i) {
+        c.use_lane(i + 1);
+        XG_CUDA(cudaEventRecord(guard.ev, c.stream));
+        c.use_lane(0);
+        XG_CUDA(cudaStreamWaitEvent(c.stream, guard.ev, 0));
+    }
+    for (int i = 0; i < m; ++i) {
+        c.use_lane(i + 1);
+        c.check_flags();
+    }
+    c.use_lane(0);
+    XG_CUDA(cudaStreamSynchronize(c.stream));
+}
+
 
 }  // namespace xg

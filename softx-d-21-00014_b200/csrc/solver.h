@@ -101,6 +101,20 @@ class Krylov : public SolverBase {
     void solve(DVec &x, DVec &b, const std::vector<double> &conv) override;
     ~Krylov() override;
 
+    // The merged BiCGStab forms (MergedPBiCGStab, PBiCGStab, MergedBiCGStab,
+    // BiCGStab) in steps, one host synchronisation apart, so that a batch of
+    // independent solves can run in lockstep on separate lanes (solve() is
+    // these steps on one system): begin() launches r0 = b - A x and posts
+    // rho0; started() (after the lane's stream is synchronised) tests it;
+    // step() launches one iteration up to its residual and posts it;
+    // stepped() tests it and launches the rest of the iteration, or the final
+    // x update. started()/stepped() return true when the solve is finished.
+    bool steppable() const { return !pcg && !rbicgstab; }
+    void begin(DVec &x, DVec &b, const std::vector<double> &conv);
+    bool started();
+    void step();
+    bool stepped();
+
   private:
     bool check(const double *res, const double *res0, std::vector<double> &iconv);
     void apply_M(DVec &out, DVec &in);
@@ -108,7 +122,13 @@ class Krylov : public SolverBase {
     void solve_pcg(DVec &x, DVec &b, const std::vector<double> &conv);
     void solve_rbicgstab(DVec &x, DVec &b, const std::vector<double> &conv);
     void upload_iconv(const std::vector<double> &iconv);
-    std::map<std::tuple<const void *, const void *, bool>, MGraph> graphs_;
+    // per (out, in, in.zero, lane): a graph's kernels carry its lane's scratch
+    std::map<std::tuple<const void *, const void *, bool, int>, MGraph> graphs_;
+    // state of the merged BiCGStab solve between its steps
+    struct Run {
+        DVec *x = nullptr, *b = nullptr, *pa = nullptr, *sa = nullptr;
+        std::vector<double> iconv, rho0, res;
+    } run_;
 };
 
 // The solver hierarchy of XAMG_solver_create* (construct_solver_hierarchy,
@@ -123,5 +143,15 @@ struct SolverHierarchy {
     void build(const Params &P, const HCsr &hA_, const DCsr *A_, int nv, HierCache *cache);
     void solve(DVec &x, DVec &b);
 };
+
+// Solves independent systems together (XAMG_b200_solver_solve_batch): system i
+// runs on lane i + 1 (its own stream and reduction scratch), so the systems'
+// kernels run concurrently. The merged BiCGStab forms advance in lockstep:
+// every round launches one iteration of each unfinished system, then the host
+// synchronises the lanes once and tests each residual. Other methods run to
+// the end on their lane. The lanes start after the work already queued on
+// lane 0, and lane 0 waits for all of them before the call returns.
+void solve_batch(const std::vector<SolverHierarchy *> &hs, const std::vector<DVec *> &xs,
+                 const std::vector<DVec *> &bs);
 
 }  // namespace xg

@@ -59,7 +59,7 @@ EXT_SYMBOLS = [
     "XAMG_b200_write_system", "XAMG_b200_solver_hierarchy_save",
     "XAMG_b200_matrix_hierarchy_load", "XAMG_b200_gemm_bf16", "XAMG_b200_mlp_create",
     "XAMG_b200_mlp_destroy", "XAMG_b200_mlp_predict", "XAMG_b200_mlp_train_step",
-    "XAMG_b200_mlp_gradients", "XAMG_b200_mlp_params",
+    "XAMG_b200_mlp_gradients", "XAMG_b200_mlp_params", "XAMG_b200_solver_solve_batch",
 ]
 
 
@@ -195,6 +195,7 @@ def lib():
                                               C.POINTER(C.c_double)]),
         "XAMG_b200_mlp_params": (C.c_int, [C.c_size_t, vp, C.c_int, C.POINTER(u64)]),
         "XAMG_b200_matrix_hierarchy_load": (C.c_int, [C.c_size_t, C.c_char_p]),
+        "XAMG_b200_solver_solve_batch": (C.c_int, [C.c_int, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -444,6 +445,17 @@ class Vector:
         p = C.c_void_p()
         call("XAMG_b200_vector_device_ptr", self.h, C.byref(p))
         return p.value
+
+
+def solve_batch(solvers, xs, bs):
+    """XAMG_b200_solver_solve_batch: solver i solves x_i from b_i, all systems
+    together (each on its own stream, the merged BiCGStab forms in lockstep)."""
+    m = len(solvers)
+    nv = np.array([x.nv for x in xs], np.uint16)
+    xh = np.array([x.h for x in xs], np.uint64)
+    bh = np.array([b.h for b in bs], np.uint64)
+    sh = np.array([S.h for S in solvers], np.uint64)
+    call("XAMG_b200_solver_solve_batch", m, _ptr(nv), _ptr(xh), _ptr(bh), _ptr(sh))
 
 
 class Solver:
