@@ -305,7 +305,7 @@ def roofline(X, torch, stream, S, n, nv, args, which=3, reps=50):
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "spmv_traffic.json")
     if os.path.exists(tfile):
-        t = json.load(open(tfile)).get(f"{args.workload}_which{which}_nv{nv}")
+        t = json.load(open(tfile)).get(f"{args.workload}_n{n}_which{which}_nv{nv}")
         if t:
             traffic = t["dram_bytes_per_launch"]
     return {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
