@@ -273,10 +273,15 @@ __device__ __forceinline__ void ld_x(const FX *p, FX (&o)[VK]) {
 template <int VK>
 constexpr int spmv_min_blocks() { return 4 * VK; }
 
+#ifndef XG_SPMV_UNROLL
+#define XG_SPMV_UNROLL 4
+#endif
+constexpr int SPMV_UNROLL = XG_SPMV_UNROLL;
+
 template <typename F, typename FX, typename I, int NV, int VK>
 __device__ __forceinline__ void row_sum(F (&y)[VK], uint32_t len, uint64_t i, int k0, const I *cl,
                                         const F *vl, const FX *x) {
-#pragma unroll 4
+#pragma unroll SPMV_UNROLL
     for (uint32_t j = 0; j < len; ++j) {
         const uint64_t c = col_at<I>(cl[j], i);
         const F av = vl[j];
@@ -1193,18 +1198,37 @@ __global__ void __launch_bounds__(CT)
 }
 
 // Dense y = A_inv b (dense_matvec.inl:109-117): thread (i, k) accumulates
-// over j in order.
+// over j in order. The inverse is stored column by column (element (i, j)
+// at j*n + i). A block of DT threads holds DT/NV consecutive rows; it copies
+// chunks of DJ columns of its rows and the matching DJ rows of x into shared
+// memory with coalesced loads, then every thread runs its sum over the chunk
+// from shared memory, so the sequential sums wait on shared memory rather
+// than on L2.
+constexpr int DT = 64;
+constexpr int DJ = 64;
 template <typename F, int NV>
-__global__ void __launch_bounds__(CT)
+__global__ void __launch_bounds__(DT)
     k_dense(const F *__restrict__ a, uint64_t n, const F *__restrict__ x, F *__restrict__ y) {
-    const uint64_t e = (uint64_t)blockIdx.x * CT + threadIdx.x;
-    if (e >= n * NV) return;
-    const uint64_t i = e / NV;
-    const int k = (int)(e % NV);
+    constexpr int RB = DT / NV;  // rows a block
+    __shared__ F xs[DJ * NV];
+    __shared__ F as[DJ * RB];
+    const int r = threadIdx.x / NV, k = threadIdx.x % NV;
+    const uint64_t i0 = (uint64_t)blockIdx.x * RB;
+    const uint64_t i = i0 + r;
     F acc = F(0);
-    const F *ar = a + i * n;
-    for (uint64_t j = 0; j < n; ++j) acc = add(acc, mul(__ldg(&ar[j]), x[j * NV + k]));
-    y[e] = acc;
+    for (uint64_t j0 = 0; j0 < n; j0 += DJ) {
+        const int jc = (int)(n - j0 < (uint64_t)DJ ? n - j0 : (uint64_t)DJ);
+        __syncthreads();  // the previous chunk is consumed
+        for (int t = threadIdx.x; t < jc * NV; t += DT) xs[t] = __ldg(&x[j0 * NV + t]);
+        for (int t = threadIdx.x; t < jc * RB; t += DT) {
+            const int jj = t / RB, rr = t % RB;
+            as[t] = i0 + rr < n ? __ldg(&a[(j0 + jj) * n + i0 + rr]) : F(0);
+        }
+        __syncthreads();
+        if (i < n)
+            for (int jj = 0; jj < jc; ++jj) acc = add(acc, mul(as[jj * RB + r], xs[jj * NV + k]));
+    }
+    if (i < n) y[i * NV + k] = acc;
 }
 
 }  // namespace k

@@ -50,8 +50,8 @@ void dense_apply(const F *a, uint64_t n, const F *x, F *y, int nv, cudaStream_t 
     if (n == 0) return;
     dispatch_nv(nv, [&](auto nvc) {
         constexpr int NV = decltype(nvc)::value;
-        const uint64_t m = n * NV;
-        k::k_dense<F, NV><<<(unsigned)((m + k::CT - 1) / k::CT), k::CT, 0, s>>>(a, n, x, y);
+        constexpr uint64_t RB = k::DT / NV;
+        k::k_dense<F, NV><<<(unsigned)((n + RB - 1) / RB), k::DT, 0, s>>>(a, n, x, y);
         XG_CUDA(cudaGetLastError());
         ++g_kernel_launches;
     });

@@ -360,11 +360,19 @@ struct Direct : public SolverBase {
                    "direct solver on " + std::to_string(hA.nrows) +
                        " rows (at most 16384): coarsen further (mg_max_levels, "
                        "mg_coarse_matrix_size)");
+        // stored column by column for k_dense's coalesced reads
         if (f32)
-            upload(inv, dense_inverse_f32(hA), S());
+            upload(inv, transposed(dense_inverse_f32(hA), hA.nrows), S());
         else
-            upload(inv, dense_inverse_f64(hA), S());
+            upload(inv, transposed(dense_inverse_f64(hA), hA.nrows), S());
         XG_CUDA(cudaStreamSynchronize(S()));
+    }
+    template <typename T>
+    static std::vector<T> transposed(const std::vector<T> &a, uint64_t n) {
+        std::vector<T> t(a.size());
+        for (uint64_t i = 0; i < n; ++i)
+            for (uint64_t j = 0; j < n; ++j) t[j * n + i] = a[i * n + j];
+        return t;
     }
     void solve(DVec &x, DVec &b, const std::vector<double> &) override {
         // blas2::Ax_y short-circuit on a zero-flagged input (blas2.h:309-313)

@@ -127,3 +127,81 @@ class LibraryCompute:
         self.X.call("XAMG_b200_spmv", C.byref(d), x.data_ptr(), y.data_ptr(), nv, 1,
                     self.X.stream())
         return y
+
+    def dot(self, a, c, nv):
+        """Partial (a, c) per right-hand side over this rank's rows
+        (XAMG_b200_dot, the library's fixed reduction order), as a device
+        tensor."""
+        import numpy as np
+        a, c = a.contiguous(), c.contiguous()
+        out = np.zeros(nv)
+        self.X.call("XAMG_b200_dot", a.shape[0], nv, a.data_ptr(), c.data_ptr(),
+                    out.ctypes.data, self.X.stream())
+        return self.torch.from_numpy(out).to(a.device)
+
+
+def rank_sum(dist, torch, local, world):
+    """The global sum of every rank's partial values (nv of them), added in
+    rank order on every rank, so that all ranks hold the same bits (XAMG's
+    allreduce also hands every rank one result, shm_allreduce.h:37-164)."""
+    if world == 1:
+        return local
+    parts = [torch.empty_like(local) for _ in range(world)]
+    dist.all_gather(parts, local.contiguous())
+    s = parts[0].clone()
+    for p in parts[1:]:
+        s = s + p
+    return s
+
+
+def bicgstab(plan, b, x, nv, compute, dist, torch, dinv, rel_tol=1e-8, max_iters=1000):
+    """Jacobi-preconditioned BiCGStab (the iteration of
+    merged_pbicgstab.inl:44-225 with M = D^-1) on this rank's rows: one halo
+    exchange per SpMV, and the dot products as per-rank partial sums (the
+    compute object's `dot`) added in rank order (rank_sum). b, x: [nl][nv]
+    tensors of this rank's rows; dinv: [nl] inverse diagonal. Converged
+    right-hand sides are frozen (their alpha and omega set to zero), as XAMG's
+    per-RHS iconv mask does (merged_bicgstab.inl:173-174,198-199). Returns x,
+    the iteration count and the final relative residuals."""
+    W = plan.world
+
+    def gdot(a, c):
+        return rank_sum(dist, torch, compute.dot(a, c, nv), W)
+
+    def A(v):
+        return spmv(plan, v, nv, compute, dist, torch)
+
+    def M(v):
+        return v * dinv[:, None]
+
+    r0 = b - A(x)
+    r, p = r0.clone(), r0.clone()
+    rho = gdot(r0, r0)
+    res0 = rho.clone()
+    iconv = torch.ones(nv, dtype=b.dtype, device=b.device)
+    it = 0
+    rel = torch.ones_like(rho)
+    while it < max_iters:
+        it += 1
+        p_ = M(p)
+        v = A(p_)
+        alpha = rho / gdot(r0, v) * iconv
+        s = r - alpha * v
+        s_ = M(s)
+        t = A(s_)
+        omega = gdot(t, s) / gdot(t, t) * iconv
+        x = x + alpha * p_ + omega * s_
+        r = s - omega * t
+        rr = gdot(r, r)
+        rel = torch.sqrt(rr / res0)
+        conv = (rel <= rel_tol) | (res0 == 0)
+        iconv = iconv * (~conv).to(iconv.dtype)
+        if bool(conv.all()):
+            break
+        rho_new = gdot(r0, r)
+        beta = (rho_new / rho) * (alpha / omega)
+        beta = torch.where(iconv > 0, beta, torch.zeros_like(beta))
+        p = r + beta * (p - omega * v)
+        rho = rho_new
+    return x, it, rel
+
