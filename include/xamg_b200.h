@@ -133,6 +133,14 @@ int XAMG_b200_solver_level_info(size_t sid, int level, int which, uint64_t *nrow
                                 uint64_t *ncols, uint64_t *nnz, int *col_bytes, int *val_f32,
                                 uint16_t *hash, double *min_eig, double *max_eig);
 
+/* The SpMV launch shapes the autotuner (parameter gpu_spmv_tune, default 1)
+ * picked for level matrix `which` (no counterpart): 24 codes, index
+ * [value type is float][x type is float][log2 nv]; 0 = not tuned (yet), else
+ * 1 + 2 * (right-hand sides a thread: 0 the default of 2 for double and 4 for
+ * float x, 1 the other one) + (staging buffers - 1). Only SpMVs without dot
+ * products are tuned; every shape gives the same results bit for bit. */
+int XAMG_b200_solver_level_tuned(size_t sid, int level, int which, uint8_t *codes);
+
 /* Copy level matrix `which` back from the device exactly as stored: row
  * pointers (u32), narrowed columns (col_bytes each), values (float/double). */
 int XAMG_b200_solver_level_download(size_t sid, int level, int which, uint32_t *row, void *col,

@@ -45,13 +45,13 @@ struct MatObj {
     HCsr h;
     bool constructed = false;
     HierCache hcache;  // host multigrid hierarchies built for this matrix
-    // device copies keyed by the narrowing switch
+    // device copies keyed by the narrowing switch and the tuning switch
     std::map<int, std::unique_ptr<DCsr>> dev;
-    const DCsr *device(int narrow) {
-        auto &p = dev[narrow];
+    const DCsr *device(int narrow, bool tune) {
+        auto &p = dev[narrow * 2 + (tune ? 1 : 0)];
         if (!p) {
             p.reset(new DCsr());
-            upload_csr(h, *p, false, narrow, ctx().stream);
+            upload_csr(h, *p, false, narrow, ctx().stream, tune);
         }
         return p.get();
     }
@@ -513,7 +513,7 @@ static void build_solver(SolverObj &so, const Params &P, int nv) {
     XG_REQUIRE(m.constructed, XAMG_ERR_INVALID_ARG, "matrix not constructed");
     SolverCfg c = resolve_cfg(P.get("solver"), "solver");
     const int narrow = c.gpu_index_compress;
-    const DCsr *A = m.device(narrow);
+    const DCsr *A = m.device(narrow, c.gpu_spmv_tune != 0);
     so.sh.reset(new SolverHierarchy());
     so.sh->build(P, m.h, A, nv, &m.hcache);
     so.nv = nv;
@@ -567,6 +567,7 @@ int XAMG_solver_renew_params(XAMG_param_id pid, XAMG_solver_id sid) {
         auto keep_gpu = [](SolverCfg &dst, const SolverCfg &src) {
             dst.gpu_index_compress = src.gpu_index_compress;
             dst.gpu_hsgs_rows = src.gpu_hsgs_rows;
+            dst.gpu_spmv_tune = src.gpu_spmv_tune;
         };
         keep_gpu(c, sh.root->cfg);
         sh.root->cfg = c;
@@ -853,6 +854,14 @@ int XAMG_b200_solver_level_info(size_t sid, int level, int which, uint64_t *nrow
         MultiGrid *mg = solver_mg(sid);
         if (min_eig) *min_eig = mg ? mg->L[level].min_eig : 0.0;
         if (max_eig) *max_eig = mg ? mg->L[level].max_eig : 0.0;
+    });
+}
+
+int XAMG_b200_solver_level_tuned(size_t sid, int level, int which, uint8_t *codes) {
+    return guarded([&] {
+        XG_REQUIRE(codes, XAMG_ERR_INVALID_ARG, "null array");
+        const DCsr &d = level_matrix(sid, level, which);
+        std::memcpy(codes, &d.tuned[0][0][0], 24);
     });
 }
 

@@ -138,6 +138,13 @@ struct DCsr {
     // largest number of entries in one tile of 256/nv rows, per nv = 1..32
     // (index log2 nv); 0 = not known yet
     uint32_t tile_max[6] = {0, 0, 0, 0, 0, 0};
+    // SpMV autotuning (library-owned matrices, gpu_spmv_tune): the launch
+    // shape measured fastest for the SpMVs without dot products, per
+    // [value type is float][x type is float][log2 nv]: 0 = not tuned yet,
+    // else 1 + (right-hand sides a thread: 0 default, 1 alternative) * 2 +
+    // (staging buffers - 1)
+    bool tune_on = false;
+    mutable uint8_t tuned[2][2][6] = {};
 
     template <typename F>
     k::CsrArgs<F> args() const {
@@ -153,7 +160,9 @@ struct DCsr {
 // stores signed 16-bit offsets col - row (col_bytes = -2) for square
 // matrices whose columns need more than 16 bits but whose entries all lie
 // within 32767 of the diagonal.
-void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s);
+// tune: let the SpMVs without dot products on this matrix pick their launch
+// shape by measurement (gpu_spmv_tune).
+void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s, bool tune = false);
 void download_csr(const DCsr &d, uint32_t *row, void *col, void *val);
 
 template <typename T>

@@ -209,7 +209,8 @@ template void axpy_k<float>(float *, const float *, const double *, uint64_t, in
 // CSR upload with XAMG's narrowing (matrix_block::assemble, matrix.h:78-93:
 // hash from encode_hash, values converted to float when reduced).
 // ---------------------------------------------------------------------------
-void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s) {
+void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s, bool tune) {
+    d.tune_on = tune;
     d.nrows = h.nrows;
     d.ncols = h.ncols;
     d.nnz = h.nnz();

@@ -231,7 +231,7 @@ struct Hsgs : public SolverBase {
             od.row[i + 1] = (uint32_t)od.col.size();
         }
         upload_csr(dg, Adiag, f32, cfg.gpu_index_compress, S());
-        upload_csr(od, Aoff, f32, cfg.gpu_index_compress, S());
+        upload_csr(od, Aoff, f32, cfg.gpu_index_compress, S(), cfg.gpu_spmv_tune != 0);
         upload(boff, off, S());
         if (f32)
             upload(d, inv_diag_f32(hA, false), S());
@@ -488,6 +488,7 @@ void MultiGrid::build(const HCsr &A0, const DCsr *A0dev, const Params &P, const 
                                                   : cfg.mg_reduced_precision != 0;
     full32 = (cfg.gpu_precond_f32 == 1) && role == "preconditioner";
     const int narrow = cfg.gpu_index_compress;
+    const bool tune = cfg.gpu_spmv_tune != 0;
     L.clear();
     L.resize(nl);
     for (int l = 0; l < nl; ++l) {
@@ -496,7 +497,7 @@ void MultiGrid::build(const HCsr &A0, const DCsr *A0dev, const Params &P, const 
         lv.tf32 = reduced;
         lv.min_eig = HH.lv[l].min_eig;
         lv.max_eig = HH.lv[l].max_eig;
-        if (l >= 1 || full32) upload_csr(HH.lv[l].A, lv.A, lv.f32, narrow, S());
+        if (l >= 1 || full32) upload_csr(HH.lv[l].A, lv.A, lv.f32, narrow, S(), tune);
         if (l + 1 < nl) {
             // R = P^T (hypre_base.inl:400-401, transpose.inl:31-108)
             const HCsr &Ph = HH.lv[l].P;
@@ -517,8 +518,8 @@ void MultiGrid::build(const HCsr &A0, const DCsr *A0dev, const Params &P, const 
                     R.val[pos[c]] = Ph.val[j];
                     ++pos[c];
                 }
-            upload_csr(Ph, lv.P, lv.tf32, narrow, S());
-            upload_csr(R, lv.R, lv.tf32, narrow, S());
+            upload_csr(Ph, lv.P, lv.tf32, narrow, S(), tune);
+            upload_csr(R, lv.R, lv.tf32, narrow, S(), tune);
         }
         const uint64_t nrow = HH.lv[l].A.nrows;
         if (l == 0) {
@@ -540,6 +541,7 @@ void MultiGrid::build(const HCsr &A0, const DCsr *A0dev, const Params &P, const 
         SolverCfg pc = resolve_cfg(P.get("pre_smoother", l), "pre_smoother");
         SolverCfg qc = resolve_cfg(P.get("post_smoother", l), "post_smoother");
         pc.gpu_index_compress = qc.gpu_index_compress = cfg.gpu_index_compress;
+        pc.gpu_spmv_tune = qc.gpu_spmv_tune = cfg.gpu_spmv_tune;
         pre.push_back(make_smoother(pc, "pre_smoother", Al, HH.lv[l].A, L[l].f32, nv,
                                     L[l].min_eig, L[l].max_eig));
         post.push_back(make_smoother(qc, "post_smoother", Al, HH.lv[l].A, L[l].f32, nv,

@@ -98,7 +98,8 @@ static int resident_blocks(Kern kern, int threads, size_t smem) {
 // the tiles still go to the canonical B = min(ntiles, 1184) blocks, which the
 // grid's blocks run in turn; without, the grid's blocks take the tiles.
 template <typename F, typename FX, typename I, int NV, int VK, int NRED, class Epi>
-static void launch_vk(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s) {
+static void launch_vk(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s,
+                      uint32_t nbuf_force = 0) {
     constexpr uint32_t LIMIT1 = (96u * 1024u - 64u) / (uint32_t)(sizeof(F) + sizeof(I));
     constexpr int NT = k::CT / VK;
     auto kern = k::k_spmv<F, FX, I, NV, VK, NRED, Epi>;
@@ -115,7 +116,7 @@ static void launch_vk(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s
     int res = res1;
     if (2 * one <= (size_t)stage_buffer_bytes<F, I>(LIMIT1)) {
         const int res2 = resident_blocks(kern, NT, 2 * one);
-        if (res2 >= res1) {
+        if ((nbuf_force == 0 && res2 >= res1) || nbuf_force == 2) {
             nbuf = 2;
             res = res2;
         }
@@ -132,6 +133,60 @@ static void launch_vk(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s
     ++g_kernel_launches;
 }
 
+// Autotuner of the SpMVs without dot products: the right-hand sides a thread
+// carries (2 or 4; the alternative of spmv_vk's choice) and the staging
+// buffers (1 or 2) are timed with CUDA events on the caller's x into a
+// scratch y (EStore), once per matrix, precision and nv, outside any graph
+// capture; the fastest is kept in the matrix (DCsr::tuned). Every candidate
+// sums each (row, right-hand side) in the same CSR order, so the choice never
+// changes a result.
+template <typename FX, int NV>
+constexpr int spmv_vk_alt() {
+    constexpr int d = k::spmv_vk<FX, NV>();
+    constexpr int a = d == 2 ? 4 : d == 4 ? 2 : d;
+    return a <= NV ? a : d;
+}
+
+template <typename F, typename FX, typename I, int NV>
+static uint8_t autotune(const DCsr &A, const FX *x, cudaStream_t s) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    XG_CUDA(cudaStreamIsCapturing(s, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return 0;
+    constexpr int VD = k::spmv_vk<FX, NV>();
+    constexpr int VA = spmv_vk_alt<FX, NV>();
+    DevBuf y(A.nrows * (uint64_t)NV * sizeof(F));
+    k::EStore<F, NV> e{{}, y.as<F>()};
+    cudaEvent_t e0, e1;
+    XG_CUDA(cudaEventCreate(&e0));
+    XG_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    uint8_t code = 1;
+    for (int alt = 0; alt < (VA != VD ? 2 : 1); ++alt)
+        for (uint32_t nb = 1; nb <= 2; ++nb) {
+            auto run = [&] {
+                if (alt)
+                    launch_vk<F, FX, I, NV, VA, 0>(A, x, e, s, nb);
+                else
+                    launch_vk<F, FX, I, NV, VD, 0>(A, x, e, s, nb);
+            };
+            run();
+            XG_CUDA(cudaEventRecord(e0, s));
+            for (int r = 0; r < 3; ++r) run();
+            XG_CUDA(cudaEventRecord(e1, s));
+            XG_CUDA(cudaEventSynchronize(e1));
+            float ms = 0;
+            XG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < best) {
+                best = ms;
+                code = (uint8_t)(1 + alt * 2 + (nb - 1));
+            }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    XG_CUDA(cudaStreamSynchronize(s));
+    return code;
+}
+
 // Vector loads of x need x aligned to VK elements; library vectors always are
 // (cudaMalloc). The entry points that take a caller's x (CALLER_X) fall back
 // to one right-hand side per thread for an x that is not (same results, same
@@ -145,6 +200,22 @@ template <typename F, typename FX, typename I, int NV, int NRED, bool CALLER_X =
 static void launch(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s) {
     if (A.nrows == 0) return;
     constexpr int VK = k::spmv_vk<FX, NV>();
+    if constexpr (NRED == 0 && NV > 1) {
+        if (A.tune_on && (uintptr_t)x % (4 * sizeof(FX)) == 0) {
+            int l = 0;
+            while ((1 << l) < NV) ++l;
+            uint8_t &t = A.tuned[sizeof(F) == 4][sizeof(FX) == 4][l];
+            if (!t) t = autotune<F, FX, I, NV>(A, x, s);
+            if (t) {
+                const uint32_t nb = (uint32_t)((t - 1) % 2 + 1);
+                if ((t - 1) / 2)
+                    launch_vk<F, FX, I, NV, spmv_vk_alt<FX, NV>(), NRED>(A, x, epi, s, nb);
+                else
+                    launch_vk<F, FX, I, NV, VK, NRED>(A, x, epi, s, nb);
+                return;
+            }
+        }
+    }
     constexpr uintptr_t ALIGN = VK * sizeof(FX);
     constexpr bool SHORT4 = sizeof(FX) == 8 && VK == 2 && NV >= 4 && NRED == 0;
     if (SHORT4 && A.nnz < 16 * A.nrows && (uintptr_t)x % (4 * sizeof(FX)) == 0) {

@@ -60,6 +60,7 @@ EXT_SYMBOLS = [
     "XAMG_b200_matrix_hierarchy_load", "XAMG_b200_gemm_bf16", "XAMG_b200_mlp_create",
     "XAMG_b200_mlp_destroy", "XAMG_b200_mlp_predict", "XAMG_b200_mlp_train_step",
     "XAMG_b200_mlp_gradients", "XAMG_b200_mlp_params", "XAMG_b200_solver_solve_batch",
+    "XAMG_b200_solver_level_tuned",
 ]
 
 
@@ -196,6 +197,7 @@ def lib():
         "XAMG_b200_mlp_params": (C.c_int, [C.c_size_t, vp, C.c_int, C.POINTER(u64)]),
         "XAMG_b200_matrix_hierarchy_load": (C.c_int, [C.c_size_t, C.c_char_p]),
         "XAMG_b200_solver_solve_batch": (C.c_int, [C.c_int, vp, vp, vp, vp]),
+        "XAMG_b200_solver_level_tuned": (C.c_int, [C.c_size_t, C.c_int, C.c_int, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -501,6 +503,13 @@ class Solver:
              C.byref(nz), C.byref(cb), C.byref(f32), C.byref(hsh), C.byref(mn), C.byref(mx))
         return dict(nrows=nr.value, ncols=nc.value, nnz=nz.value, col_bytes=cb.value,
                     f32=bool(f32.value), hash=hsh.value, min_eig=mn.value, max_eig=mx.value)
+
+    def level_tuned(self, level, which):
+        """The autotuner's launch-shape codes of a level matrix, as a
+        [2][2][6] array (value float, x float, log2 nv)."""
+        out = np.zeros(24, np.uint8)
+        call("XAMG_b200_solver_level_tuned", self.h, level, which, _ptr(out))
+        return out.reshape(2, 2, 6)
 
     def level_download(self, level, which):
         info = self.level_info(level, which)

@@ -285,3 +285,29 @@ def test_rbicgstab_with_amg(gpu, oracle, method, f32):
     assert sg["conv"].tolist() == so["conv"].tolist()
     assert sg["rel_res"].tobytes() == so["rel_res"].tobytes()
     assert xg.tobytes() == xo.tobytes()
+
+
+@pytest.mark.parametrize("stencil,edge,nv,f32", [(27, 14, 8, True), (27, 12, 4, False),
+                                                 (7, 20, 16, True), (7, 18, 32, False)])
+def test_autotuned_spmv_same_results(gpu, stencil, edge, nv, f32):
+    """The SpMV autotuner (gpu_spmv_tune) only picks launch shapes: a solve
+    with it equals the solve without it bit for bit, and it has recorded a
+    choice for the matrices the preconditioner's SpMVs ran on."""
+    row, col, val = gpu.generate_diffusion(stencil, edge, edge, edge, 1.0, 1.0, 4)
+    n = len(row) - 1
+    b = np.random.default_rng(9).uniform(-1, 1, n * nv)
+    sm = {"method": "Chebyshev", "polynomial_order": 2}
+    out = {}
+    for tune in (0, 1):
+        params = {"solver": {"method": "MergedPBiCGStab", "max_iters": 100,
+                             "rel_tolerance": 1e-8, "abs_tolerance": 0, "gpu_spmv_tune": tune},
+                  "preconditioner": dict(MG_BASE, method="MultiGrid",
+                                         gpu_precond_f32=1 if f32 else 0, gpu_spmv_tune=tune),
+                  "pre_smoother": sm, "post_smoother": dict(sm),
+                  "coarse_grid_solver": {"method": "Direct"}}
+        x, st, S = gpu_solve(gpu, row, col, val, nv, params, b)
+        out[tune] = (x, st)
+        codes = S.level_tuned(1, 3)
+        assert (codes.any()) == bool(tune)
+    assert out[0][0].tobytes() == out[1][0].tobytes()
+    assert out[0][1]["iters"] == out[1][1]["iters"]
