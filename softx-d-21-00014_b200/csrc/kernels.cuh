@@ -392,11 +392,13 @@ __device__ __forceinline__ uint32_t stage_shift(const T *arr, uint32_t j0) {
 // Tiles are dealt round-robin to B canonical blocks (tile t to block t % B);
 // physical block p runs canonical blocks p, p + gridDim.x, ... in turn, so a
 // grid of the blocks that fit the GPU at once covers any B. Without dot
-// products B is simply the grid size.
+// products B is simply the grid size, and the tiles may be dealt in runs of
+// `run` consecutive tiles (run q to block q % gridDim.x), so that a block's
+// successive tiles share columns in its SM's L1.
 template <typename F, typename FX, typename I, int NV, int VK, int NRED, class Epi>
 __global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
     k_spmv(CsrArgs<F> A, const FX *__restrict__ x, Epi epi, RedArgs ra, uint32_t cap,
-           uint32_t nbuf, uint32_t B) {
+           uint32_t nbuf, uint32_t B, uint32_t run = 1) {
     constexpr int G = NV / VK;
     constexpr int R = CT / NV;
     constexpr int NR = NRED > 0 ? NRED : 1;
@@ -414,10 +416,16 @@ __global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
     const uint64_t ntiles = (n + R - 1) / R;
     // tile after t in this physical block's sequence (ntiles: none)
     auto next_tile = [&](uint64_t t) -> uint64_t {
+        if constexpr (NRED == 0) {
+            if ((t + 1) % run != 0 && t + 1 < ntiles) return t + 1;
+            const uint64_t q = (t / run + gridDim.x) * run;
+            return q < ntiles ? q : ntiles;
+        }
         if (t + B < ntiles) return t + B;
         const uint64_t c = t % B + gridDim.x;
         return c < B ? c : ntiles;
     };
+    const uint64_t first = NRED == 0 ? (uint64_t)blockIdx.x * run : (uint64_t)blockIdx.x;
     F acc[VK][NR];
 #pragma unroll
     for (int v = 0; v < VK; ++v)
@@ -452,9 +460,9 @@ __global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
         if (vb) bulk_g2s(vdst, vsrc, vb, m);
         if (cb) bulk_g2s(cdst, csrc, cb, m);
     };
-    if (threadIdx.x == 0) issue(blockIdx.x);
+    if (threadIdx.x == 0) issue(first);
 
-    for (uint64_t tile = blockIdx.x; tile < ntiles;) {
+    for (uint64_t tile = first; tile < ntiles;) {
         const uint64_t tnext = next_tile(tile);
         const uint64_t r0 = tile * R;
         const uint64_t r1 = r0 + R < n ? r0 + R : n;

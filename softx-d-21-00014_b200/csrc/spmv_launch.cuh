@@ -99,7 +99,7 @@ static int resident_blocks(Kern kern, int threads, size_t smem) {
 // grid's blocks run in turn; without, the grid's blocks take the tiles.
 template <typename F, typename FX, typename I, int NV, int VK, int NRED, class Epi>
 static void launch_vk(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s,
-                      uint32_t nbuf_force = 0) {
+                      uint32_t nbuf_force = 0, uint32_t run = 1) {
     constexpr uint32_t LIMIT1 = (96u * 1024u - 64u) / (uint32_t)(sizeof(F) + sizeof(I));
     constexpr int NT = k::CT / VK;
     auto kern = k::k_spmv<F, FX, I, NV, VK, NRED, Epi>;
@@ -125,21 +125,32 @@ static void launch_vk(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s
     const uint64_t R = k::CT / NV;
     const uint64_t ntiles = (A.nrows + R - 1) / R;
     const uint64_t wave = (uint64_t)res * (uint64_t)ctx().sms;
+    if (NRED > 0 || run < 1) run = 1;
     const uint32_t B = NRED > 0 ? (uint32_t)k::canon_blocks(A.nrows, NV)
-                                : (uint32_t)std::min<uint64_t>(ntiles, wave);
+                                : (uint32_t)std::min<uint64_t>((ntiles + run - 1) / run, wave);
     const uint32_t P = (uint32_t)std::min<uint64_t>(B, wave);
-    kern<<<P, NT, smem, s>>>(A.args<F>(), x, epi, ctx().red(), cap, nbuf, B);
+    kern<<<P, NT, smem, s>>>(A.args<F>(), x, epi, ctx().red(), cap, nbuf, B, run);
     XG_CUDA(cudaGetLastError());
     ++g_kernel_launches;
 }
 
 // Autotuner of the SpMVs without dot products: the right-hand sides a thread
-// carries (2 or 4; the alternative of spmv_vk's choice) and the staging
-// buffers (1 or 2) are timed with CUDA events on the caller's x into a
-// scratch y (EStore), once per matrix, precision and nv, outside any graph
-// capture; the fastest is kept in the matrix (DCsr::tuned). Every candidate
-// sums each (row, right-hand side) in the same CSR order, so the choice never
-// changes a result.
+// carries (2 or 4; the alternative of spmv_vk's choice), the staging buffers
+// (1 or 2) and the run of consecutive tiles a block takes (1, 4 or 16) are
+// timed with CUDA events on the caller's x into a scratch y (EStore), once
+// per matrix, precision and nv, outside any graph capture; the fastest is
+// kept in the matrix (DCsr::tuned). Every candidate sums each (row,
+// right-hand side) in the same CSR order, so the choice never changes a
+// result.
+constexpr uint32_t TUNE_RUNS[3] = {1, 4, 16};
+struct Tuned {
+    int alt;
+    uint32_t nbuf, run;
+};
+inline Tuned tuned_shape(uint8_t code) {
+    const int c = code - 1;
+    return Tuned{c / 6, (uint32_t)((c / 3) % 2 + 1), TUNE_RUNS[c % 3]};
+}
 template <typename FX, int NV>
 constexpr int spmv_vk_alt() {
     constexpr int d = k::spmv_vk<FX, NV>();
@@ -162,25 +173,26 @@ static uint8_t autotune(const DCsr &A, const FX *x, cudaStream_t s) {
     float best = 1e30f;
     uint8_t code = 1;
     for (int alt = 0; alt < (VA != VD ? 2 : 1); ++alt)
-        for (uint32_t nb = 1; nb <= 2; ++nb) {
-            auto run = [&] {
-                if (alt)
-                    launch_vk<F, FX, I, NV, VA, 0>(A, x, e, s, nb);
-                else
-                    launch_vk<F, FX, I, NV, VD, 0>(A, x, e, s, nb);
-            };
-            run();
-            XG_CUDA(cudaEventRecord(e0, s));
-            for (int r = 0; r < 3; ++r) run();
-            XG_CUDA(cudaEventRecord(e1, s));
-            XG_CUDA(cudaEventSynchronize(e1));
-            float ms = 0;
-            XG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-            if (ms < best) {
-                best = ms;
-                code = (uint8_t)(1 + alt * 2 + (nb - 1));
+        for (uint32_t nb = 1; nb <= 2; ++nb)
+            for (int ri = 0; ri < 3; ++ri) {
+                auto go = [&] {
+                    if (alt)
+                        launch_vk<F, FX, I, NV, VA, 0>(A, x, e, s, nb, TUNE_RUNS[ri]);
+                    else
+                        launch_vk<F, FX, I, NV, VD, 0>(A, x, e, s, nb, TUNE_RUNS[ri]);
+                };
+                go();
+                XG_CUDA(cudaEventRecord(e0, s));
+                for (int r = 0; r < 3; ++r) go();
+                XG_CUDA(cudaEventRecord(e1, s));
+                XG_CUDA(cudaEventSynchronize(e1));
+                float ms = 0;
+                XG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                if (ms < best) {
+                    best = ms;
+                    code = (uint8_t)(1 + alt * 6 + (nb - 1) * 3 + ri);
+                }
             }
-        }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     XG_CUDA(cudaStreamSynchronize(s));
@@ -207,11 +219,12 @@ static void launch(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s) {
             uint8_t &t = A.tuned[sizeof(F) == 4][sizeof(FX) == 4][l];
             if (!t) t = autotune<F, FX, I, NV>(A, x, s);
             if (t) {
-                const uint32_t nb = (uint32_t)((t - 1) % 2 + 1);
-                if ((t - 1) / 2)
-                    launch_vk<F, FX, I, NV, spmv_vk_alt<FX, NV>(), NRED>(A, x, epi, s, nb);
+                const Tuned c = tuned_shape(t);
+                if (c.alt)
+                    launch_vk<F, FX, I, NV, spmv_vk_alt<FX, NV>(), NRED>(A, x, epi, s, c.nbuf,
+                                                                        c.run);
                 else
-                    launch_vk<F, FX, I, NV, VK, NRED>(A, x, epi, s, nb);
+                    launch_vk<F, FX, I, NV, VK, NRED>(A, x, epi, s, c.nbuf, c.run);
                 return;
             }
         }
