@@ -136,9 +136,9 @@ int XAMG_b200_solver_level_info(size_t sid, int level, int which, uint64_t *nrow
 /* The SpMV launch shapes the autotuner (parameter gpu_spmv_tune, default 1)
  * picked for level matrix `which` (no counterpart): 24 codes, index
  * [value type is float][x type is float][log2 nv]; 0 = not tuned (yet), else
- * 1 + 6 * (right-hand sides a thread: 0 the default of 2 for double and 4 for
- * float x, 1 the other one) + 3 * (staging buffers - 1) + (consecutive tiles
- * a block takes: 0 one, 1 four, 2 sixteen). Only SpMVs without dot products
+ * 1 + 9 * (right-hand sides a thread: 0 the default of 2 for double and 4 for
+ * float x, 1 the other one) + 3 * (staging: 0 one buffer, 1 two, 2 none) +
+ * (consecutive tiles a block takes: 0 one, 1 four, 2 sixteen). Only SpMVs without dot products
  * are tuned; every shape gives the same results bit for bit. */
 int XAMG_b200_solver_level_tuned(size_t sid, int level, int which, uint8_t *codes);
 

@@ -109,7 +109,8 @@ static void launch_vk(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s
                                      (int)stage_buffer_bytes<F, I>(LIMIT1)));
         big_smem = true;
     }
-    const uint32_t cap = std::min(tile_max(A, NV, s), LIMIT1);
+    // nbuf_force 3: no staging (every tile reads global memory)
+    const uint32_t cap = nbuf_force == 3 ? 0u : std::min(tile_max(A, NV, s), LIMIT1);
     const size_t one = stage_buffer_bytes<F, I>(cap);
     const int res1 = resident_blocks(kern, NT, one);
     uint32_t nbuf = 1;
@@ -136,7 +137,9 @@ static void launch_vk(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s
 
 // Autotuner of the SpMVs without dot products: the right-hand sides a thread
 // carries (2 or 4; the alternative of spmv_vk's choice), the staging buffers
-// (1 or 2) and the run of consecutive tiles a block takes (1, 4 or 16) are
+// (1, 2, or none: tiles read from global memory, for small matrices where the
+// copy's round trip is not hidden) and the run of consecutive tiles a block
+// takes (1, 4 or 16) are
 // timed with CUDA events on the caller's x into a scratch y (EStore), once
 // per matrix, precision and nv, outside any graph capture; the fastest is
 // kept in the matrix (DCsr::tuned). Every candidate sums each (row,
@@ -149,7 +152,7 @@ struct Tuned {
 };
 inline Tuned tuned_shape(uint8_t code) {
     const int c = code - 1;
-    return Tuned{c / 6, (uint32_t)((c / 3) % 2 + 1), TUNE_RUNS[c % 3]};
+    return Tuned{c / 9, (uint32_t)((c / 3) % 3 + 1), TUNE_RUNS[c % 3]};
 }
 template <typename FX, int NV>
 constexpr int spmv_vk_alt() {
@@ -173,7 +176,7 @@ static uint8_t autotune(const DCsr &A, const FX *x, cudaStream_t s) {
     float best = 1e30f;
     uint8_t code = 1;
     for (int alt = 0; alt < (VA != VD ? 2 : 1); ++alt)
-        for (uint32_t nb = 1; nb <= 2; ++nb)
+        for (uint32_t nb = 1; nb <= 3; ++nb)
             for (int ri = 0; ri < 3; ++ri) {
                 auto go = [&] {
                     if (alt)
@@ -190,7 +193,7 @@ static uint8_t autotune(const DCsr &A, const FX *x, cudaStream_t s) {
                 XG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
                 if (ms < best) {
                     best = ms;
-                    code = (uint8_t)(1 + alt * 6 + (nb - 1) * 3 + ri);
+                    code = (uint8_t)(1 + alt * 9 + (nb - 1) * 3 + ri);
                 }
             }
     cudaEventDestroy(e0);
