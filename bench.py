@@ -37,7 +37,7 @@ sys.path.insert(0, os.path.join(ROOT, "softx-d-21-00014_b200"))
 WORKLOADS = {
     "amg27": dict(desc="27-pt var-kappa Q1 FE 128^3, nv=8, PBiCGStab + AMG V(1,1) Chebyshev-2",
                   stencil=27, grid=128, sigma=1.0, aniso=1.0, nv=8, smoother="Chebyshev",
-                  order=2),
+                  order=2, bf16_levels=2),
     "poisson32": dict(desc="7-pt Poisson 32^3 (cube.inl), nv=1, MergedPBiCGStab + Jacobi",
                       stencil=0, grid=32, sigma=0.0, aniso=1.0, nv=1, smoother=None, order=0),
     "aniso192": dict(desc="27-pt var-kappa Q1 FE 192^3, kappa=exp(N(0,4)), 4:1 z-anisotropy, nv=32, "
@@ -66,7 +66,9 @@ def params_for(w, reduced):
         sm["max_iters"] = w["sweeps"]
     # plain: XAMG's FP64 method with XAMG's index narrowing. chosen: the whole
     # multigrid preconditioner (finest level included) in FP32 with 2-byte
-    # column offsets where they fit; the outer iteration stays FP64.
+    # column offsets where they fit, and on the workloads where it measured
+    # faster the finest levels' matrix values stored in BF16 (bf16_levels);
+    # the outer iteration stays FP64.
     prec = {"method": "MultiGrid", "max_iters": 1, "mg_agg_num_levels": 0,
             "mg_strength_threshold": 0.25, "mg_coarsening_type": 8,
             "mg_interpolation_type": 6, "mg_coarse_matrix_size": 500,
@@ -74,7 +76,8 @@ def params_for(w, reduced):
     solver = {"method": "MergedPBiCGStab", "max_iters": 500, "rel_tolerance": 1e-8,
               "abs_tolerance": 0, "gpu_index_compress": 1}
     if reduced:
-        prec.update(gpu_precond_f32=1, gpu_index_compress=2)
+        prec.update(gpu_precond_f32=1, gpu_index_compress=2,
+                    gpu_level_bf16=w.get("bf16_levels", 0))
         solver.update(gpu_index_compress=2)
     return {"solver": solver, "preconditioner": prec,
             "pre_smoother": sm, "post_smoother": dict(sm),
@@ -247,7 +250,9 @@ def run_ours(args, w):
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": res[chosen]["ms"] / args.steps,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64 outer / f32 preconditioner" if chosen == "chosen" else "f64",
+        "dtype": ("f64 outer / f32 preconditioner" +
+                  (f" (bf16 values on the {w['bf16_levels']} finest levels)"
+                   if w.get("bf16_levels") else "")) if chosen == "chosen" else "f64",
         "data": "synthetic",
         "config": {"workload": w["desc"], "rows": n, "nnz": int(len(col)), "nv": nv,
                    "rhs_per_gpu_per_step": nv, "tolerance": 1e-8,
@@ -282,7 +287,8 @@ def roofline(X, torch, stream, S, n, nv, args, which=3, reps=50):
     bytes per launch: values and narrowed columns once, row pointers, x read
     and y written once (x's reuse across rows is served by the caches)."""
     A0 = S.level_csr(0, which)
-    esz = 4 if A0.val_f32 else 8
+    esz = 4 if A0.val_f32 else 8                    # x and y elements
+    vsz = {0: 8, 1: 4, 2: 2}[A0.val_f32]             # stored values (2: BF16)
     dt = torch.float32 if A0.val_f32 else torch.float64
     xd = torch.empty(n * nv, dtype=dt, device="cuda").uniform_(-1, 1)
     yd = torch.empty(n * nv, dtype=dt, device="cuda")
@@ -297,15 +303,15 @@ def roofline(X, torch, stream, S, n, nv, args, which=3, reps=50):
         e1.record(stream)
     e1.synchronize()
     ms = e0.elapsed_time(e1) / reps
-    alg = A0.nnz * (esz + abs(A0.col_bytes)) + (n + 1) * 4 + 2 * n * nv * esz
+    alg = A0.nnz * (vsz + abs(A0.col_bytes)) + (n + 1) * 4 + 2 * n * nv * esz
     achieved = alg / (ms * 1e-3) / 1e9
     peak, peak_kind = peaks()
     kname = f"k_spmv<{'float' if esz == 4 else 'double'}> level 0, EStore, nv={nv}, " \
-            f"col_bytes={A0.col_bytes}"
+            f"col_bytes={A0.col_bytes}" + (", BF16 values" if vsz == 2 else "")
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "spmv_traffic.json")
     if os.path.exists(tfile):
-        t = json.load(open(tfile)).get(f"{args.workload}_n{n}_which{which}_nv{nv}")
+        t = json.load(open(tfile)).get(f"{args.workload}_n{n}_which{which}_nv{nv}_v{vsz}")
         if t:
             traffic = t["dram_bytes_per_launch"]
     return {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,

@@ -44,7 +44,9 @@ int XAMG_b200_build_info(char *buf, size_t len);
  * col_bytes = -2: signed 16-bit offsets col - row, a form with no
  * counterpart in the reference, used for square matrices whose entries all
  * lie within 32767 of the diagonal (parameter gpu_index_compress = 2).
- * Row pointers are 32-bit. Values are double (val_f32 = 0) or float. */
+ * Row pointers are 32-bit. Values are double (val_f32 = 0), float (1), or
+ * BF16 with float arithmetic (2: the FP32 cycle levels that parameter
+ * gpu_level_bf16 selects; no counterpart in the reference). */
 typedef struct {
     uint64_t nrows, ncols, nnz;
     const uint32_t *row;
@@ -128,7 +130,7 @@ int XAMG_b200_solver_nlevels(size_t sid);
 /* Shape of level matrix `which` (0 = A, 1 = R, 2 = P, 3 = the operator the
  * multigrid cycle applies on the level: A, or on level 0 the FP32 copy when
  * gpu_precond_f32 is set) as uploaded: sizes, narrowed column width, value
- * type, XAMG hash, eigenvalue estimates. */
+ * type (val_f32 as in XAMG_b200_csr), XAMG hash, eigenvalue estimates. */
 int XAMG_b200_solver_level_info(size_t sid, int level, int which, uint64_t *nrows,
                                 uint64_t *ncols, uint64_t *nnz, int *col_bytes, int *val_f32,
                                 uint16_t *hash, double *min_eig, double *max_eig);

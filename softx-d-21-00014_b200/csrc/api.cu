@@ -136,7 +136,10 @@ struct BorrowedCsr {
         d.ncols = A->ncols;
         d.nnz = A->nnz;
         d.col_bytes = A->col_bytes;
+        XG_REQUIRE(A->val_f32 >= 0 && A->val_f32 <= 2, XAMG_ERR_INVALID_ARG,
+                   "val_f32 must be 0, 1 or 2");
         d.f32 = A->val_f32 != 0;
+        d.bf16 = A->val_f32 == 2;
         d.row.p = (void *)A->row;
         d.col.p = (void *)A->col;
         d.val.p = (void *)A->val;
@@ -849,7 +852,7 @@ int XAMG_b200_solver_level_info(size_t sid, int level, int which, uint64_t *nrow
         if (ncols) *ncols = d.ncols;
         if (nnz) *nnz = d.nnz;
         if (col_bytes) *col_bytes = d.col_bytes;
-        if (val_f32) *val_f32 = d.f32;
+        if (val_f32) *val_f32 = d.bf16 ? 2 : d.f32 ? 1 : 0;
         if (hash) *hash = d.hash;
         MultiGrid *mg = solver_mg(sid);
         if (min_eig) *min_eig = mg ? mg->L[level].min_eig : 0.0;
@@ -906,7 +909,7 @@ int XAMG_b200_solver_level_csr(size_t sid, int level, int which, XAMG_b200_csr *
         out->col = d.col.p;
         out->val = d.val.p;
         out->col_bytes = d.col_bytes;
-        out->val_f32 = d.f32;
+        out->val_f32 = d.bf16 ? 2 : d.f32 ? 1 : 0;
     });
 }
 

@@ -133,6 +133,7 @@ struct DCsr {
     uint64_t nrows = 0, ncols = 0, nnz = 0;
     int col_bytes = 4;
     bool f32 = false;
+    bool bf16 = false;  // float matrix whose values are stored in BF16
     uint16_t hash = 0;
     DevBuf row, col, val;
     // largest number of entries in one tile of 256/nv rows, per nv = 1..32
@@ -163,7 +164,10 @@ struct DCsr {
 // within 32767 of the diagonal.
 // tune: let the SpMVs without dot products on this matrix pick their launch
 // shape by measurement (gpu_spmv_tune).
-void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s, bool tune = false);
+// bf16 (with f32): store the values rounded to float and then to BF16
+// (round to nearest even), the arithmetic staying in float.
+void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s, bool tune = false,
+                bool bf16 = false);
 void download_csr(const DCsr &d, uint32_t *row, void *col, void *val);
 
 template <typename T>

@@ -27,6 +27,7 @@
 // replay it exactly.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -278,13 +279,23 @@ constexpr int spmv_min_blocks() { return 4 * VK; }
 #endif
 constexpr int SPMV_UNROLL = XG_SPMV_UNROLL;
 
-template <typename F, typename FX, typename I, int NV, int VK>
+// A stored matrix value in the arithmetic type F: the value itself, or a
+// BF16 value widened exactly to float.
+template <typename F, typename V>
+__device__ __forceinline__ F val_as(V v) {
+    if constexpr (std::is_same<V, __nv_bfloat16>::value)
+        return (F)__bfloat162float(v);
+    else
+        return (F)v;
+}
+
+template <typename F, typename FX, typename I, int NV, int VK, typename V = F>
 __device__ __forceinline__ void row_sum(F (&y)[VK], uint32_t len, uint64_t i, int k0, const I *cl,
-                                        const F *vl, const FX *x) {
+                                        const V *vl, const FX *x) {
 #pragma unroll SPMV_UNROLL
     for (uint32_t j = 0; j < len; ++j) {
         const uint64_t c = col_at<I>(cl[j], i);
-        const F av = vl[j];
+        const F av = val_as<F, V>(vl[j]);
         FX xv[VK];
         ld_x<FX, VK>(x + c * NV + k0, xv);
 #pragma unroll
@@ -386,7 +397,9 @@ __device__ __forceinline__ uint32_t stage_shift(const T *arr, uint32_t j0) {
 
 // Kernel with dynamic shared memory: nbuf (1 or 2) buffers, each of cap
 // entries of values and columns plus 32 bytes of alignment slack per array;
-// tiles with more entries read global memory directly.
+// tiles with more entries read global memory directly. V is the type the
+// values are stored in: F, or BF16 for an FP32 level stored in BF16 (the
+// arithmetic stays in F).
 // CT/VK threads; thread p carries row slot p/(NV/VK) and right-hand sides
 // k0 = (p % (NV/VK))*VK .. k0+VK-1 (x aligned to VK elements).
 // Tiles are dealt round-robin to B canonical blocks (tile t to block t % B);
@@ -395,7 +408,8 @@ __device__ __forceinline__ uint32_t stage_shift(const T *arr, uint32_t j0) {
 // products B is simply the grid size, and the tiles may be dealt in runs of
 // `run` consecutive tiles (run q to block q % gridDim.x), so that a block's
 // successive tiles share columns in its SM's L1.
-template <typename F, typename FX, typename I, int NV, int VK, int NRED, class Epi>
+template <typename F, typename FX, typename I, int NV, int VK, int NRED, class Epi,
+          typename V = F>
 __global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
     k_spmv(CsrArgs<F> A, const FX *__restrict__ x, Epi epi, RedArgs ra, uint32_t cap,
            uint32_t nbuf, uint32_t B, uint32_t run = 1) {
@@ -404,13 +418,13 @@ __global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
     constexpr int NR = NRED > 0 ? NRED : 1;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t mbar[2];
-    const uint32_t VB = ((cap * (uint32_t)sizeof(F) + 32u) + 15u) & ~15u;
+    const uint32_t VB = ((cap * (uint32_t)sizeof(V) + 32u) + 15u) & ~15u;
     const uint32_t BB = VB + (((cap * (uint32_t)sizeof(I) + 32u) + 15u) & ~15u);
     const uint32_t CAP = cap;
     const int rt = threadIdx.x / G, k0 = (threadIdx.x % G) * VK;
     const uint32_t *__restrict__ row = A.row;
     const I *__restrict__ col = (const I *)A.col;
-    const F *__restrict__ val = A.val;
+    const V *__restrict__ val = (const V *)A.val;
     const uint64_t n = A.n;
     const uint64_t nnz = n ? row[n] : 0;
     const uint64_t ntiles = (n + R - 1) / R;
@@ -449,11 +463,11 @@ __global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
         unsigned char *buf = smem_raw + (size_t)(n_issued % nbuf) * BB;
         uint64_t *m = &mbar[n_issued % nbuf];
         ++n_issued;
-        const F *vsrc;
-        F *vdst;
+        const V *vsrc;
+        V *vdst;
         const I *csrc;
         I *cdst;
-        const uint32_t vb = stage_range<F>((F *)buf, val, nnz, j0, j1, vsrc, vdst);
+        const uint32_t vb = stage_range<V>((V *)buf, val, nnz, j0, j1, vsrc, vdst);
         const uint32_t cb = stage_range<I>((I *)(buf + VB), col, nnz, j0, j1, csrc, cdst);
         mbar_arrive_expect(m, vb + cb);  // releases the plain-load writes above
         fence_proxy_async_smem();
@@ -469,7 +483,7 @@ __global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
         const uint32_t tj0 = __ldg(&row[r0]), tj1 = __ldg(&row[r1]);
         bool staged = tj1 - tj0 <= CAP;
         if (nbuf == 2 && threadIdx.x == 0) issue(tnext);
-        const F *sv = nullptr;
+        const V *sv = nullptr;
         const I *sc = nullptr;
         if (staged) {
             const uint32_t b = n_used % nbuf;
@@ -477,7 +491,7 @@ __global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
             if (!mbar_wait(&mbar[b], (n_used / nbuf) & 1u)) timed_out = true;
             ++n_used;
             const unsigned char *buf = smem_raw + (size_t)b * BB;
-            sv = (const F *)buf + stage_shift<F>(val, tj0);
+            sv = (const V *)buf + stage_shift<V>(val, tj0);
             sc = (const I *)(buf + VB) + stage_shift<I>(col, tj0);
             staged = !timed_out;
         }
@@ -488,9 +502,10 @@ __global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
             for (int v = 0; v < VK; ++v) y[v] = epi.init(i, k0 + v);
             const uint32_t j0 = __ldg(&row[i]), j1 = __ldg(&row[i + 1]);
             if (staged)
-                row_sum<F, FX, I, NV, VK>(y, j1 - j0, i, k0, sc + (j0 - tj0), sv + (j0 - tj0), x);
+                row_sum<F, FX, I, NV, VK, V>(y, j1 - j0, i, k0, sc + (j0 - tj0), sv + (j0 - tj0),
+                                             x);
             else
-                row_sum<F, FX, I, NV, VK>(y, j1 - j0, i, k0, col + j0, val + j0, x);
+                row_sum<F, FX, I, NV, VK, V>(y, j1 - j0, i, k0, col + j0, val + j0, x);
 #pragma unroll
             for (int v = 0; v < VK; ++v) epi.store(i, k0 + v, y[v], acc[v]);
         }

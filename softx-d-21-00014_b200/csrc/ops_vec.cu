@@ -209,8 +209,10 @@ template void axpy_k<float>(float *, const float *, const double *, uint64_t, in
 // CSR upload with XAMG's narrowing (matrix_block::assemble, matrix.h:78-93:
 // hash from encode_hash, values converted to float when reduced).
 // ---------------------------------------------------------------------------
-void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s, bool tune) {
+void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s, bool tune,
+                bool bf16) {
     d.tune_on = tune;
+    d.bf16 = f32 && bf16;
     d.nrows = h.nrows;
     d.ncols = h.ncols;
     d.nnz = h.nnz();
@@ -260,7 +262,12 @@ void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s, bo
         upload(d.col, c, s);
         XG_CUDA(cudaStreamSynchronize(s));
     }
-    if (f32) {
+    if (d.bf16) {
+        std::vector<__nv_bfloat16> v(h.val.size());
+        for (size_t i = 0; i < v.size(); ++i) v[i] = __float2bfloat16_rn((float)h.val[i]);
+        upload(d.val, v, s);
+        XG_CUDA(cudaStreamSynchronize(s));
+    } else if (f32) {
         std::vector<float> v(h.val.size());
         for (size_t i = 0; i < v.size(); ++i) v[i] = (float)h.val[i];
         upload(d.val, v, s);

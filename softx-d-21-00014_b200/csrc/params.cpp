@@ -75,6 +75,7 @@ static const std::map<std::string, KeyInfo> &dictionary() {
         {"gpu_hsgs_rows", {'I', ""}},
         {"gpu_graph", {'I', ""}},
         {"gpu_spmv_tune", {'I', ""}},
+        {"gpu_level_bf16", {'I', ""}},
         {"gpu_seed", {'I', ""}},
     };
     return d;
@@ -319,6 +320,7 @@ SolverCfg resolve_cfg(const PList &l, const std::string &role) {
     c.gpu_hsgs_rows = l.get_i("gpu_hsgs_rows", 32);
     c.gpu_graph = l.get_i("gpu_graph", 1);
     c.gpu_spmv_tune = l.get_i("gpu_spmv_tune", 1);
+    c.gpu_level_bf16 = l.get_i("gpu_level_bf16", 0);
     c.gpu_seed = l.get_i("gpu_seed", 0);
     return c;
 }

@@ -80,6 +80,7 @@ struct SolverCfg {
     int gpu_hsgs_rows = 32;     // target rows per hybrid Gauss-Seidel block
     int gpu_graph = 1;          // replay preconditioner applications as CUDA graphs
     int gpu_spmv_tune = 1;      // SpMV launch shapes picked by measurement
+    int gpu_level_bf16 = 0;     // finest FP32 cycle levels whose matrix values are BF16
     int gpu_seed = 0;           // seed of the host setup's random choices
 };
 

@@ -97,25 +97,26 @@ static int resident_blocks(Kern kern, int threads, size_t smem) {
 // Grid: as many blocks as fit the GPU at once (one wave). With dot products
 // the tiles still go to the canonical B = min(ntiles, 1184) blocks, which the
 // grid's blocks run in turn; without, the grid's blocks take the tiles.
-template <typename F, typename FX, typename I, int NV, int VK, int NRED, class Epi>
+template <typename F, typename FX, typename I, int NV, int VK, int NRED, typename V = F,
+          class Epi>
 static void launch_vk(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s,
                       uint32_t nbuf_force = 0, uint32_t run = 1) {
-    constexpr uint32_t LIMIT1 = (96u * 1024u - 64u) / (uint32_t)(sizeof(F) + sizeof(I));
+    constexpr uint32_t LIMIT1 = (96u * 1024u - 64u) / (uint32_t)(sizeof(V) + sizeof(I));
     constexpr int NT = k::CT / VK;
-    auto kern = k::k_spmv<F, FX, I, NV, VK, NRED, Epi>;
+    auto kern = k::k_spmv<F, FX, I, NV, VK, NRED, Epi, V>;
     static bool big_smem = false;  // one flag per instantiation
     if (!big_smem) {
         XG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)stage_buffer_bytes<F, I>(LIMIT1)));
+                                     (int)stage_buffer_bytes<V, I>(LIMIT1)));
         big_smem = true;
     }
     // nbuf_force 3: no staging (every tile reads global memory)
     const uint32_t cap = nbuf_force == 3 ? 0u : std::min(tile_max(A, NV, s), LIMIT1);
-    const size_t one = stage_buffer_bytes<F, I>(cap);
+    const size_t one = stage_buffer_bytes<V, I>(cap);
     const int res1 = resident_blocks(kern, NT, one);
     uint32_t nbuf = 1;
     int res = res1;
-    if (2 * one <= (size_t)stage_buffer_bytes<F, I>(LIMIT1)) {
+    if (2 * one <= (size_t)stage_buffer_bytes<V, I>(LIMIT1)) {
         const int res2 = resident_blocks(kern, NT, 2 * one);
         if ((nbuf_force == 0 && res2 >= res1) || nbuf_force == 2) {
             nbuf = 2;
@@ -161,7 +162,7 @@ constexpr int spmv_vk_alt() {
     return a <= NV ? a : d;
 }
 
-template <typename F, typename FX, typename I, int NV>
+template <typename F, typename FX, typename I, int NV, typename V>
 static uint8_t autotune(const DCsr &A, const FX *x, cudaStream_t s) {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     XG_CUDA(cudaStreamIsCapturing(s, &cs));
@@ -180,9 +181,9 @@ static uint8_t autotune(const DCsr &A, const FX *x, cudaStream_t s) {
             for (int ri = 0; ri < 3; ++ri) {
                 auto go = [&] {
                     if (alt)
-                        launch_vk<F, FX, I, NV, VA, 0>(A, x, e, s, nb, TUNE_RUNS[ri]);
+                        launch_vk<F, FX, I, NV, VA, 0, V>(A, x, e, s, nb, TUNE_RUNS[ri]);
                     else
-                        launch_vk<F, FX, I, NV, VD, 0>(A, x, e, s, nb, TUNE_RUNS[ri]);
+                        launch_vk<F, FX, I, NV, VD, 0, V>(A, x, e, s, nb, TUNE_RUNS[ri]);
                 };
                 go();
                 XG_CUDA(cudaEventRecord(e0, s));
@@ -210,24 +211,23 @@ static uint8_t autotune(const DCsr &A, const FX *x, cudaStream_t s) {
 // and the like) takes four right-hand sides per thread: the staging buffers
 // are small enough for sixteen 64-thread blocks an SM, and the wider gathers
 // win; longer rows keep two.
-template <typename F, typename FX, typename I, int NV, int NRED, bool CALLER_X = false,
+template <typename F, typename FX, typename I, int NV, int NRED, bool CALLER_X, typename V,
           class Epi>
-static void launch(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s) {
-    if (A.nrows == 0) return;
+static void launch_v(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s) {
     constexpr int VK = k::spmv_vk<FX, NV>();
     if constexpr (NRED == 0 && NV > 1) {
         if (A.tune_on && (uintptr_t)x % (4 * sizeof(FX)) == 0) {
             int l = 0;
             while ((1 << l) < NV) ++l;
             uint8_t &t = A.tuned[sizeof(F) == 4][sizeof(FX) == 4][l];
-            if (!t) t = autotune<F, FX, I, NV>(A, x, s);
+            if (!t) t = autotune<F, FX, I, NV, V>(A, x, s);
             if (t) {
                 const Tuned c = tuned_shape(t);
                 if (c.alt)
-                    launch_vk<F, FX, I, NV, spmv_vk_alt<FX, NV>(), NRED>(A, x, epi, s, c.nbuf,
-                                                                        c.run);
+                    launch_vk<F, FX, I, NV, spmv_vk_alt<FX, NV>(), NRED, V>(A, x, epi, s,
+                                                                           c.nbuf, c.run);
                 else
-                    launch_vk<F, FX, I, NV, VK, NRED>(A, x, epi, s, c.nbuf, c.run);
+                    launch_vk<F, FX, I, NV, VK, NRED, V>(A, x, epi, s, c.nbuf, c.run);
                 return;
             }
         }
@@ -235,14 +235,30 @@ static void launch(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s) {
     constexpr uintptr_t ALIGN = VK * sizeof(FX);
     constexpr bool SHORT4 = sizeof(FX) == 8 && VK == 2 && NV >= 4 && NRED == 0;
     if (SHORT4 && A.nnz < 16 * A.nrows && (uintptr_t)x % (4 * sizeof(FX)) == 0) {
-        if constexpr (SHORT4) launch_vk<F, FX, I, NV, 4, NRED>(A, x, epi, s);
+        if constexpr (SHORT4) launch_vk<F, FX, I, NV, 4, NRED, V>(A, x, epi, s);
     } else if (VK == 1 || (uintptr_t)x % ALIGN == 0) {
-        launch_vk<F, FX, I, NV, VK, NRED>(A, x, epi, s);
+        launch_vk<F, FX, I, NV, VK, NRED, V>(A, x, epi, s);
     } else if constexpr (CALLER_X) {
-        launch_vk<F, FX, I, NV, 1, NRED>(A, x, epi, s);
+        launch_vk<F, FX, I, NV, 1, NRED, V>(A, x, epi, s);
     } else {
         throw Error(XAMG_ERR_INTERNAL, "library vector not aligned for the SpMV gather");
     }
+}
+
+// FP32 matrices may store their values in BF16 (DCsr::bf16; gpu_level_bf16):
+// the kernel then widens each value to float as it reads it.
+template <typename F, typename FX, typename I, int NV, int NRED, bool CALLER_X = false,
+          class Epi>
+static void launch(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s) {
+    if (A.nrows == 0) return;
+    if constexpr (std::is_same<F, float>::value) {
+        if (A.bf16) {
+            launch_v<F, FX, I, NV, NRED, CALLER_X, __nv_bfloat16>(A, x, epi, s);
+            return;
+        }
+    }
+    XG_REQUIRE(!A.bf16, XAMG_ERR_INTERNAL, "BF16 values on a double matrix");
+    launch_v<F, FX, I, NV, NRED, CALLER_X, F>(A, x, epi, s);
 }
 
 template <typename F, int NV, int NRED, class Epi>

@@ -502,7 +502,8 @@ class Solver:
         call("XAMG_b200_solver_level_info", self.h, level, which, C.byref(nr), C.byref(nc),
              C.byref(nz), C.byref(cb), C.byref(f32), C.byref(hsh), C.byref(mn), C.byref(mx))
         return dict(nrows=nr.value, ncols=nc.value, nnz=nz.value, col_bytes=cb.value,
-                    f32=bool(f32.value), hash=hsh.value, min_eig=mn.value, max_eig=mx.value)
+                    f32=bool(f32.value), bf16=f32.value == 2, hash=hsh.value, min_eig=mn.value,
+                    max_eig=mx.value)
 
     def level_tuned(self, level, which):
         """The autotuner's launch-shape codes of a level matrix, as a
@@ -514,10 +515,16 @@ class Solver:
     def level_download(self, level, which):
         info = self.level_info(level, which)
         row = np.zeros(info["nrows"] + 1, np.uint32)
-        col = np.zeros(info["nnz"], {1: np.uint8, 2: np.uint16, 4: np.uint32}[info["col_bytes"]])
-        val = np.zeros(info["nnz"], np.float32 if info["f32"] else np.float64)
+        col = np.zeros(info["nnz"], {1: np.uint8, 2: np.uint16, 4: np.uint32,
+                                     -2: np.int16}[info["col_bytes"]])
+        if info["bf16"]:  # BF16 bits, widened to float32 below
+            val = np.zeros(info["nnz"], np.uint16)
+        else:
+            val = np.zeros(info["nnz"], np.float32 if info["f32"] else np.float64)
         call("XAMG_b200_solver_level_download", self.h, level, which, _ptr(row), _ptr(col),
              _ptr(val))
+        if info["bf16"]:
+            val = (val.astype(np.uint32) << 16).view(np.float32)
         return row, col, val, info
 
     def save_hierarchy(self, path):

@@ -111,3 +111,35 @@ def test_fp64_27pt_diag_first(gpu, oracle, nv):
     xh, y0, y, ya = run_level_spmv(gpu, S, 0, 0, row, col, val, nv, False, seed=nv)
     assert y.tobytes() == oracle.csr_ax_y(row, col, val, xh, nv).tobytes()
     assert ya.tobytes() == oracle.csr_ax_y(row, col, val, xh, nv, axpy_y=y0).tobytes()
+
+
+def bf16_round(v):
+    """float64 values rounded to float32 and then to BF16 (round to nearest
+    even), returned as float32: what an FP32 level stored in BF16 holds."""
+    b = np.asarray(v, np.float64).astype(np.float32).view(np.uint32)
+    b = (b + (((b >> 16) & 1) + 0x7FFF)) & 0xFFFF0000
+    return b.astype(np.uint32).view(np.float32)
+
+
+@pytest.mark.parametrize("nv", [1, 8, 32])
+def test_bf16_cycle_operators_bit_exact(gpu, oracle, nv):
+    """gpu_level_bf16 = 2: the two finest FP32 cycle operators store BF16
+    values and compute in float. Their SpMVs must equal the oracle's float
+    row sums over the BF16-rounded values bit for bit."""
+    row, col, val = gpu.generate_diffusion(27, 14, 13, 12, 1.0, 1.0, 3)
+    params = {"solver": {"method": "MergedPBiCGStab", "rel_tolerance": 1e-8, "max_iters": 5,
+                         "gpu_index_compress": 2},
+              "preconditioner": {"method": "MultiGrid", "mg_max_levels": 3,
+                                 "gpu_precond_f32": 1, "gpu_index_compress": 2,
+                                 "gpu_level_bf16": 2},
+              "pre_smoother": {"method": "Chebyshev"}, "post_smoother": {"method": "Chebyshev"}}
+    _, _, _, S = solver_on(gpu, row, col, val, nv, params)
+    assert S.level_info(0, 3)["bf16"] and S.level_info(1, 3)["bf16"]
+    assert not S.level_info(2, 3)["bf16"]
+    xh, y0, y, ya = run_level_spmv(gpu, S, 0, 3, row, col, val, nv, True, seed=nv)
+    vb = bf16_round(val)
+    assert y.tobytes() == oracle.csr_ax_y(row, col, vb, xh, nv).tobytes()
+    assert ya.tobytes() == oracle.csr_ax_y(row, col, vb, xh, nv, axpy_y=y0).tobytes()
+    r1, c1, v1, info = S.level_download(1, 3)
+    x1, y01, y1, ya1 = run_level_spmv(gpu, S, 1, 3, r1, c1, v1, nv, True, seed=nv + 1)
+    assert y1.tobytes() == oracle.csr_ax_y(r1, c1.astype(np.uint32), v1, x1, nv).tobytes()
