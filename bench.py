@@ -432,33 +432,46 @@ def run_batch(args, w):
     call per step (chosen: FP32 preconditioner, every system on its own
     stream, lockstep iterations) against one XAMG_solver_solve2 call per
     system (the same solvers, and XAMG's plain FP64 method). Synthetic
-    systems: edges and nv drawn from a seeded generator."""
+    systems: edges and nv drawn from a seeded generator. Under torchrun the
+    systems are shared out among the ranks (largest first, to the least
+    loaded rank; replicas.assign_systems) with no data-path collective: the
+    total work is fixed, so the scaling is strong, and every time is the
+    maximum over ranks."""
     import torch
     import xamg_b200 as X
-    X.init()
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    X.init(device=local)
     stream = torch.cuda.ExternalStream(X.stream())
     rng = np.random.default_rng(3)
     m = w["systems"]
     edges = rng.choice(np.arange(16, 97, 8), m)
     nvs = rng.choice([1, 4, 16], m)
+    owner = replicas.assign_systems((edges.astype(float) ** 3 * nvs).tolist(), ws)
     t0 = time.time()
     sysm = []
     for i in range(m):
         e, nv = int(edges[i]), int(nvs[i])
+        n = e ** 3
+        b = rng.uniform(-1, 1, n * nv)  # drawn on every rank: the same b whatever the split
+        if owner[i] != rank:
+            continue
         row, col, val = X.generate_diffusion(7, e, e, e, w["sigma"], 1.0, 100 + i)
-        n = len(row) - 1
         M = X.Matrix(row, col, val)
-        b = rng.uniform(-1, 1, n * nv)
         bv, xv = X.Vector(n, nv), X.Vector(n, nv)
         bv.upload(b)
         xv.set(0.0)
         S = X.Solver(M, X.Params(batch_params(True)), xv, bv)
         P = X.Solver(M, X.Params(batch_params(False)), xv, bv)
-        sysm.append(dict(M=M, b=b, bv=bv, xv=xv, S=S, P=P, n=n, nv=nv,
+        sysm.append(dict(M=M, b=b, bv=bv, xv=xv, S=S, P=P, n=n, nv=nv, edge=e,
                          bh=torch.from_numpy(b).pin_memory(),
                          xh=torch.empty(n * nv, dtype=torch.float64).pin_memory(),
                          row=row, col=col, val=val))
-    setup_s = time.time() - t0
+    setup_s = max_over_ranks(time.time() - t0, ws)
     total_rhs = int(nvs.sum())
     Ss = [d["S"] for d in sysm]
     xs = [d["xv"] for d in sysm]
@@ -483,6 +496,7 @@ def run_batch(args, w):
     def timed(kind, K, e2e=False):
         for _ in range(args.warmup):
             step(kind)
+        barrier(ws)
         torch.cuda.synchronize()
         k0 = X.kernel_launches()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -492,9 +506,14 @@ def run_batch(args, w):
                 step(kind, e2e)
             e1.record(stream)
         e1.synchronize()
-        return e0.elapsed_time(e1) / K, (X.kernel_launches() - k0) // K
+        torch.cuda.synchronize()
+        barrier(ws)
+        ms = max_over_ranks(e0.elapsed_time(e1) / K, ws)
+        launches = replicas.sum_over_ranks((X.kernel_launches() - k0) // K) if ws > 1 \
+            else (X.kernel_launches() - k0) // K
+        return ms, int(launches)
 
-    with ClockSampler(0) as cs:
+    with ClockSampler(local) as cs:
         ms_batch, launches = timed("batch", args.steps)
     ms_single, _ = timed("single", args.steps)
     ms_plain, _ = timed("plain", max(1, args.steps // 2))
@@ -509,28 +528,39 @@ def run_batch(args, w):
         Xs, Bs = d["xh"].numpy().reshape(d["n"], d["nv"]), d["b"].reshape(d["n"], d["nv"])
         worst = max(worst, float((np.linalg.norm(Bs - A @ Xs, axis=0) /
                                   np.linalg.norm(Bs, axis=0)).max()))
+    worst = max_over_ranks(worst, ws)
+    it_min = -max_over_ranks(-min(iters), ws)
+    it_max = max_over_ranks(max(iters), ws)
     big = int(np.argmax([d["n"] * d["nv"] for d in sysm]))
     rf = roofline(X, torch, stream, sysm[big]["S"], sysm[big]["n"], sysm[big]["nv"], args)
-    rf["kernel"] += f" (largest system: {int(edges[big])}^3, nv={int(nvs[big])})"
+    rf["kernel"] += f" (largest system: {sysm[big]['edge']}^3, nv={sysm[big]['nv']})"
+    clocks = cs.summary()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
+    vec_bytes = int(sum(int(e) ** 3 * int(v) * 8 for e, v in zip(edges, nvs)))
     return {
-        "metric": "ms/RHS to 1e-8 residual: batch solve vs one solve per call on 1 B200",
-        "value": ms_batch / total_rhs, "unit": "ms/RHS", "n_gpus": 1, "steps": args.steps,
+        "metric": "ms/RHS to 1e-8 residual: batch solve vs one solve per call",
+        "value": ms_batch / total_rhs, "unit": "ms/RHS", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_batch, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64 outer / f32 preconditioner",
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64 outer / f32 preconditioner",
         "data": "synthetic",
-        "config": {"workload": w["desc"], "systems": m, "rows": int(sum(d["n"] for d in sysm)),
+        "config": {"workload": w["desc"], "systems": m,
+                   "rows": int(sum(int(e) ** 3 for e in edges)),
                    "rhs_per_step": total_rhs, "edges": edges.tolist(), "nv": nvs.tolist(),
+                   "systems_per_rank": [owner.count(r) for r in range(ws)],
                    "tolerance": 1e-8, "l2": "inputs larger than L2 (all systems' matrices)"},
-        "iters": {"min": min(iters), "max": max(iters), "mean": float(np.mean(iters))},
+        "iters": {"min": int(it_min), "max": int(it_max)},
         "one_call_per_system_ms_per_rhs": ms_single / total_rhs,
         "plain_fp64_ms_per_rhs": ms_plain / total_rhs,
         "batch_vs_one_call_speedup": ms_single / ms_batch,
         "chosen_vs_fp64_speedup": ms_plain / ms_batch,
         "true_rel_residual": worst,
         "e2e": {"value": ms_e2e / total_rhs, "unit": "ms/RHS",
-                "h2d_bytes_per_step": int(sum(d["n"] * d["nv"] * 8 for d in sysm)),
-                "d2h_bytes_per_step": int(sum(d["n"] * d["nv"] * 8 for d in sysm))},
-        "gpu_launches": int(launches), "roofline": rf, "clocks": cs.summary(),
+                "h2d_bytes_per_step": vec_bytes, "d2h_bytes_per_step": vec_bytes},
+        "gpu_launches": launches, "roofline": rf, "clocks": clocks,
         "setup_s": setup_s,
     }
 

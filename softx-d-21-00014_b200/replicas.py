@@ -28,6 +28,22 @@ def rhs_blocks(total_blocks, world, rank):
     return list(range(start, start + base + (1 if rank < extra else 0)))
 
 
+def assign_systems(work, world):
+    """Rank of each independent system: largest work first, each to the
+    rank with the least work so far (ties to the lower rank). Every rank
+    computes the same assignment from the same work list, so no message is
+    needed."""
+    if world < 1:
+        raise ValueError("world must be at least 1")
+    load = [0.0] * world
+    owner = [0] * len(work)
+    for i in sorted(range(len(work)), key=lambda j: (-work[j], j)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        owner[i] = r
+        load[r] += work[i]
+    return owner
+
+
 def _device(dist):
     return "cuda" if dist.get_backend() == "nccl" else "cpu"
 

@@ -82,6 +82,27 @@ def test_rhs_blocks_partition():
         replicas.rhs_blocks(4, 2, 2)
 
 
+def test_assign_systems_balanced():
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "softx-d-21-00014_b200"))
+    import numpy as np
+    import replicas
+    rng = np.random.default_rng(3)
+    edges = rng.choice(np.arange(16, 97, 8), 64)
+    nvs = rng.choice([1, 4, 16], 64)
+    work = (edges.astype(float) ** 3 * nvs).tolist()
+    assert replicas.assign_systems(work, 1) == [0] * 64
+    for world in (2, 4, 8):
+        owner = replicas.assign_systems(work, world)
+        assert owner == replicas.assign_systems(work, world)  # deterministic
+        assert sorted(set(owner)) == list(range(world))
+        load = [sum(w for w, o in zip(work, owner) if o == r) for r in range(world)]
+        # greedy largest-first: no rank exceeds the mean by more than the largest system
+        assert max(load) <= sum(work) / world + max(work)
+    with pytest.raises(ValueError):
+        replicas.assign_systems(work, 0)
+
+
 def test_two_gloo_ranks_solve_their_own_blocks(tmp_path):
     import torch.multiprocessing as mp
     world, total_blocks, nv, n_edge = 2, 3, 2, 8
