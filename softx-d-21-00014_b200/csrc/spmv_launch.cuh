@@ -251,13 +251,14 @@ template <typename F, typename FX, typename I, int NV, int NRED, bool CALLER_X =
           class Epi>
 static void launch(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s) {
     if (A.nrows == 0) return;
-    if constexpr (std::is_same<F, float>::value) {
+    if constexpr (std::is_same<F, float>::value && std::is_same<FX, float>::value) {
         if (A.bf16) {
             launch_v<F, FX, I, NV, NRED, CALLER_X, __nv_bfloat16>(A, x, epi, s);
             return;
         }
     }
-    XG_REQUIRE(!A.bf16, XAMG_ERR_INTERNAL, "BF16 values on a double matrix");
+    XG_REQUIRE(!A.bf16, XAMG_ERR_UNSUPPORTED,
+               "BF16 matrix values need float values and a float x");
     launch_v<F, FX, I, NV, NRED, CALLER_X, F>(A, x, epi, s);
 }
 
