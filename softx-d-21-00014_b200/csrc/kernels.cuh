@@ -551,9 +551,12 @@ static __global__ void k_tile_max(const uint32_t *__restrict__ row, uint64_t n, 
     }
 }
 
-// Element-wise canonical kernel (same schedule, no matrix).
+// Element-wise canonical kernel (same schedule, no matrix). At most 64
+// registers a thread, so that four 256-thread blocks share an SM (the merged
+// group kernels with nv <= 8 take 76 registers left alone, three blocks);
+// these streaming kernels are bound by the loads in flight.
 template <typename F, int NV, int NRED, class Epi>
-__global__ void __launch_bounds__(CT) k_rows(uint64_t n, Epi epi, RedArgs ra) {
+__global__ void __launch_bounds__(CT, 4) k_rows(uint64_t n, Epi epi, RedArgs ra) {
     constexpr int R = CT / NV;
     const int rt = threadIdx.x / NV, k = threadIdx.x % NV;
     const uint64_t ntiles = (n + R - 1) / R;
