@@ -219,7 +219,8 @@ def run_ours(args, w):
         return max_over_ranks(ms, ws), X.kernel_launches() - k0, xh_pin.numpy().copy()
 
     if args.roofline_only:
-        return roofline(X, torch, stream, solvers[chosen], n, nv, args, reps=args.steps)
+        return roofline(X, torch, stream, solvers[chosen], n, nv, args,
+                        which=3 if w["smoother"] else 0, reps=args.steps)
 
     res = {}
     for name, S in solvers.items():
@@ -239,7 +240,9 @@ def run_ours(args, w):
     Xs, Bs = xh.reshape(n, nv), b.reshape(n, nv)
     true_rel = (np.linalg.norm(Bs - A @ Xs, axis=0) / np.linalg.norm(Bs, axis=0)).max()
 
-    rf = roofline(X, torch, stream, S, n, nv, args)
+    # which=3: the multigrid cycle's level-0 operator; a solver without a
+    # multigrid hierarchy (Jacobi-preconditioned configuration 1) has only A
+    rf = roofline(X, torch, stream, S, n, nv, args, which=3 if w["smoother"] else 0)
     rf64 = roofline(X, torch, stream, S, n, nv, args, which=0)
 
     total_rhs = args.steps * nv * ws
