@@ -695,6 +695,8 @@ void Krylov::run_M(DVec &out, DVec &in) {
 Krylov::~Krylov() {
     for (auto &kv : graphs_)
         if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    for (auto &kv : step_graphs_)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
 }
 
 // set_const(out, 0) then precond->solve(out, in) with conv = ones. With
@@ -706,7 +708,7 @@ Krylov::~Krylov() {
 void Krylov::apply_M(DVec &out, DVec &in) {
     out.zero = true;
     out.init = true;
-    if (!cfg.gpu_graph) {
+    if (!cfg.gpu_graph || capturing_) {
         run_M(out, in);
         return;
     }
@@ -913,12 +915,72 @@ bool Krylov::started() {
     return check(run_.rho0.data(), run_.rho0.data(), run_.iconv);
 }
 
+// With gpu_graph (default) the iteration up to its residual is recorded as
+// one CUDA graph per lane on its third call (the first two settle the
+// preconditioner's graphs, flags and launch shapes; the recording runs the
+// preconditioner's kernels inline) and replayed from then on: the same
+// kernels and the same copy of the residual to the lane's pinned slots, on
+// the same buffers, in one launch. The work vectors' flags are restored as
+// the recording left them. A step that cannot be captured runs directly.
 void Krylov::step() {
+    ++st.iters;
+    run_.pa = M ? &buf[6] : &buf[2];
+    run_.sa = M ? &buf[7] : &buf[4];
+    if (!cfg.gpu_graph) {
+        step_body();
+        return;
+    }
+    MGraph &g = step_graphs_[ctx().lane];
+    if (g.exec) {
+        XG_CUDA(cudaGraphLaunch(g.exec, S()));
+        g_kernel_launches += g.launches;
+        for (size_t i = 0; i < buf.size(); ++i) {
+            buf[i].zero = g.flags[i] & 1;
+            buf[i].init = g.flags[i] & 2;
+        }
+        return;
+    }
+    if (g.failed || g.calls++ < 2) {
+        step_body();
+        return;
+    }
+    XG_CUDA(cudaStreamSynchronize(S()));
+    XG_CUDA(cudaStreamBeginCapture(S(), cudaStreamCaptureModeThreadLocal));
+    const uint64_t l0 = g_kernel_launches;
+    cudaGraph_t graph = nullptr;
+    bool ok = true;
+    capturing_ = true;
+    try {
+        step_body();  // recorded, not run
+    } catch (...) {
+        ok = false;
+    }
+    capturing_ = false;
+    const cudaError_t e = cudaStreamEndCapture(S(), &graph);
+    if (!ok || e != cudaSuccess || !graph ||
+        cudaGraphInstantiate(&g.exec, graph, 0) != cudaSuccess) {
+        // nothing ran during the capture: run directly from now on
+        cudaGetLastError();
+        if (graph) cudaGraphDestroy(graph);
+        g.exec = nullptr;
+        g.failed = true;
+        g_kernel_launches = l0;
+        step_body();
+        return;
+    }
+    cudaGraphDestroy(graph);
+    g.launches = g_kernel_launches - l0;
+    g.flags.resize(buf.size());
+    for (size_t i = 0; i < buf.size(); ++i)
+        g.flags[i] = (uint8_t)((buf[i].zero ? 1 : 0) | (buf[i].init ? 2 : 0));
+    XG_CUDA(cudaGraphLaunch(g.exec, S()));
+}
+
+void Krylov::step_body() {
     cudaStream_t s = S();
     double *SC = sc.as<double>();
     DVec &r0 = buf[0], &r = buf[1], &p = buf[2], &v = buf[3], &s_ = buf[4], &t = buf[5],
          &p_ = buf[6], &s2 = buf[7];
-    ++st.iters;
     run_.pa = &p;
     run_.sa = &s_;
     if (M) {

@@ -87,6 +87,7 @@ struct MGraph {
     bool failed = false;    // capture not possible: always run directly
     bool out_zero = false;
     uint64_t launches = 0;  // kernels in the graph
+    std::vector<uint8_t> flags;  // step graphs: zero/init of every work vector after the step
 };
 
 class Krylov : public SolverBase {
@@ -122,8 +123,12 @@ class Krylov : public SolverBase {
     void solve_pcg(DVec &x, DVec &b, const std::vector<double> &conv);
     void solve_rbicgstab(DVec &x, DVec &b, const std::vector<double> &conv);
     void upload_iconv(const std::vector<double> &iconv);
+    void step_body();
     // per (out, in, in.zero, lane): a graph's kernels carry its lane's scratch
     std::map<std::tuple<const void *, const void *, bool, int>, MGraph> graphs_;
+    // step() as one graph per lane (the work vectors are fixed from setup on)
+    std::map<int, MGraph> step_graphs_;
+    bool capturing_ = false;  // recording step(): preconditioner runs inline
     // state of the merged BiCGStab solve between its steps
     struct Run {
         DVec *x = nullptr, *b = nullptr, *pa = nullptr, *sa = nullptr;

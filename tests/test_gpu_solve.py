@@ -261,6 +261,39 @@ def test_graph_replay_matches_direct_launches(gpu, smoother):
     assert l0 == l1
 
 
+@pytest.mark.parametrize("method,prec", [("MergedPBiCGStab", "Jacobi"),
+                                         ("PBiCGStab", "MultiGrid"),
+                                         ("MergedBiCGStab", None)])
+def test_step_graph_matches_direct_launches(gpu, oracle, method, prec):
+    """gpu_graph = 1 also records one BiCGStab iteration up to its residual as
+    a CUDA graph on its third call and replays it from the fourth. Over a
+    solve of many iterations the replayed form must give the direct launches'
+    solution, iterations and kernel count bit for bit, and match the oracle."""
+    row, col, val = gpu.generate_cube(24, 24, 24)
+    nv = 2
+    b = np.random.default_rng(5).uniform(-1, 1, (len(row) - 1) * nv)
+    out = []
+    for graph in (0, 1):
+        params = {"solver": {"method": method, "max_iters": 200, "rel_tolerance": 1e-8,
+                             "abs_tolerance": 0, "gpu_graph": graph}}
+        if prec == "Jacobi":
+            params["preconditioner"] = {"method": "Jacobi"}
+        elif prec == "MultiGrid":
+            params.update(preconditioner=dict(MG_BASE, method="MultiGrid"),
+                          pre_smoother={"method": "Jacobi"}, post_smoother={"method": "Jacobi"},
+                          coarse_grid_solver={"method": "Direct"})
+        k0 = gpu.kernel_launches()
+        x, st, S = gpu_solve(gpu, row, col, val, nv, params, b)
+        out.append((x, st, gpu.kernel_launches() - k0))
+    (x0, s0, l0), (x1, s1, l1) = out
+    assert s0["iters"] == s1["iters"] and s0["iters"] >= 5
+    assert x0.tobytes() == x1.tobytes()
+    assert l0 == l1
+    xo, so, _ = oracle_solve(oracle, S, row, col, val, nv, params, b, 1)
+    assert s1["iters"] == so["iters"]
+    assert x1.tobytes() == xo.tobytes()
+
+
 @pytest.mark.parametrize("method", ["RBiCGStab", "MergedRBiCGStab"])
 @pytest.mark.parametrize("f32", [0, 1])
 def test_rbicgstab_with_amg(gpu, oracle, method, f32):
