@@ -873,6 +873,7 @@ void Krylov::solve(DVec &x, DVec &b, const std::vector<double> &conv) {
         if (stepped()) return;
         if (st.iters >= cfg.max_iters) break;
     }
+    finish();
     XG_CUDA(cudaStreamSynchronize(S()));
 }
 
@@ -890,6 +891,7 @@ void Krylov::begin(DVec &x, DVec &b, const std::vector<double> &conv) {
     cudaStream_t s = S();
     run_.x = &x;
     run_.b = &b;
+    run_.tail = false;
     run_.iconv = conv;
     run_.rho0.assign(NV, 0.0);
     run_.res.assign(NV, 0.0);
@@ -915,22 +917,37 @@ bool Krylov::started() {
     return check(run_.rho0.data(), run_.rho0.data(), run_.iconv);
 }
 
-// With gpu_graph (default) the iteration up to its residual is recorded as
-// one CUDA graph per lane on its third call (the first two settle the
-// preconditioner's graphs, flags and launch shapes; the recording runs the
-// preconditioner's kernels inline) and replayed from then on: the same
-// kernels and the same copy of the residual to the lane's pinned slots, on
-// the same buffers, in one launch. The work vectors' flags are restored as
-// the recording left them. A step that cannot be captured runs directly.
+// The previous iteration's tail (when its residual did not converge) and
+// this iteration up to its residual. With gpu_graph (default) these are
+// recorded as one CUDA graph per (lane, tail or not, x) on the third call
+// (the first two settle the preconditioner's graphs, flags and launch
+// shapes; the recording runs the preconditioner's kernels inline) and
+// replayed from then on: the same kernels and the same copy of the residual
+// to the lane's pinned slots, on the same buffers, in one launch. The work
+// vectors' flags are restored as the recording left them. A step that
+// cannot be captured runs directly.
 void Krylov::step() {
     ++st.iters;
     run_.pa = M ? &buf[6] : &buf[2];
     run_.sa = M ? &buf[7] : &buf[4];
-    if (!cfg.gpu_graph) {
+    const bool tail = run_.tail;
+    run_.tail = false;
+    auto body = [&] {
+        if (tail) step_tail();
         step_body();
+    };
+    if (!cfg.gpu_graph) {
+        body();
         return;
     }
-    MGraph &g = step_graphs_[ctx().lane];
+    const auto key = std::make_tuple(ctx().lane, tail, run_.x->p<const void>());
+    if (step_graphs_.size() >= 32 && !step_graphs_.count(key)) {
+        // many solution vectors: start over rather than keep a graph for each
+        for (auto &kv : step_graphs_)
+            if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        step_graphs_.clear();
+    }
+    MGraph &g = step_graphs_[key];
     if (g.exec) {
         XG_CUDA(cudaGraphLaunch(g.exec, S()));
         g_kernel_launches += g.launches;
@@ -938,10 +955,11 @@ void Krylov::step() {
             buf[i].zero = g.flags[i] & 1;
             buf[i].init = g.flags[i] & 2;
         }
+        if (tail) run_.x->zero = false;
         return;
     }
     if (g.failed || g.calls++ < 2) {
-        step_body();
+        body();
         return;
     }
     XG_CUDA(cudaStreamSynchronize(S()));
@@ -951,7 +969,7 @@ void Krylov::step() {
     bool ok = true;
     capturing_ = true;
     try {
-        step_body();  // recorded, not run
+        body();  // recorded, not run
     } catch (...) {
         ok = false;
     }
@@ -965,7 +983,7 @@ void Krylov::step() {
         g.exec = nullptr;
         g.failed = true;
         g_kernel_launches = l0;
-        step_body();
+        body();
         return;
     }
     cudaGraphDestroy(graph);
@@ -1006,34 +1024,46 @@ void Krylov::step_body() {
 bool Krylov::stepped() {
     cudaStream_t s = S();
     double *SC = sc.as<double>();
-    DVec &r0 = buf[0], &r = buf[1], &p = buf[2], &v = buf[3], &s_ = buf[4], &t = buf[5];
+    DVec &p = buf[2], &s_ = buf[4];
     DVec &x = *run_.x;
     take_scalars(run_.res.data(), NV);
     const bool done = check(run_.res.data(), run_.rho0.data(), run_.iconv);
+    if (!done) {
+        run_.tail = true;  // launched by the next step() or by finish()
+        return false;
+    }
+    if (precond_form)
+        ops::x_update(n, x.p<double>(), run_.pa->p<double>(), run_.sa->p<double>(), SC, NV, s);
+    else
+        ops::x_update(n, x.p<double>(), p.p<double>(), s_.p<double>(), SC, NV, s);
+    x.zero = false;
+    return true;
+}
+
+void Krylov::finish() {
+    if (!run_.tail) return;
+    run_.tail = false;
+    step_tail();
+}
+
+// The rest of an iteration whose residual did not converge.
+void Krylov::step_tail() {
+    cudaStream_t s = S();
+    double *SC = sc.as<double>();
+    DVec &r0 = buf[0], &r = buf[1], &p = buf[2], &v = buf[3], &s_ = buf[4], &t = buf[5];
+    DVec &x = *run_.x;
     if (precond_form) {
-        if (done) {
-            ops::x_update(n, x.p<double>(), run_.pa->p<double>(), run_.sa->p<double>(), SC, NV, s);
-            x.zero = false;
-            return true;
-        }
         // x update fused with r = s - omega t; rho = (r, r0); beta
         ops::group4(n, s_.p<double>(), t.p<double>(), r0.p<double>(), r.p<double>(),
                     x.p<double>(), run_.pa->p<double>(), run_.sa->p<double>(), true, SC, NV, s);
-        x.zero = false;
         ops::p_update(n, p.p<double>(), r.p<double>(), v.p<double>(), SC, NV, s);
     } else {
-        if (done) {
-            ops::x_update(n, x.p<double>(), p.p<double>(), s_.p<double>(), SC, NV, s);
-            x.zero = false;
-            return true;
-        }
         ops::group4(n, s_.p<double>(), t.p<double>(), r0.p<double>(), r.p<double>(), nullptr,
                     nullptr, nullptr, false, SC, NV, s);
         ops::group5(n, x.p<double>(), p.p<double>(), s_.p<double>(), r.p<double>(),
                     v.p<double>(), SC, NV, s);
-        x.zero = false;
     }
-    return false;
+    x.zero = false;
 }
 
 // ===========================================================================
@@ -1167,7 +1197,12 @@ void solve_batch(const std::vector<SolverHierarchy *> &hs, const std::vector<DVe
             if (live[i]) {
                 c.use_lane(i + 1);
                 XG_CUDA(cudaStreamSynchronize(c.stream));
-                if (kr[i]->stepped() || kr[i]->st.iters >= kr[i]->cfg.max_iters) live[i] = 0;
+                if (kr[i]->stepped()) {
+                    live[i] = 0;
+                } else if (kr[i]->st.iters >= kr[i]->cfg.max_iters) {
+                    kr[i]->finish();
+                    live[i] = 0;
+                }
             }
     }
     // join: lane 0 waits for every lane; then each lane's wait-timeout flag

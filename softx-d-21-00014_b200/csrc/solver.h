@@ -107,14 +107,17 @@ class Krylov : public SolverBase {
     // independent solves can run in lockstep on separate lanes (solve() is
     // these steps on one system): begin() launches r0 = b - A x and posts
     // rho0; started() (after the lane's stream is synchronised) tests it;
-    // step() launches one iteration up to its residual and posts it;
-    // stepped() tests it and launches the rest of the iteration, or the final
-    // x update. started()/stepped() return true when the solve is finished.
+    // step() launches the rest of the previous iteration, if one is pending,
+    // and one iteration up to its residual, and posts it; stepped() tests it
+    // and launches the final x update, or leaves the rest of the iteration
+    // pending. started()/stepped() return true when the solve is finished;
+    // finish() launches a pending rest when the solve stops at max_iters.
     bool steppable() const { return !pcg && !rbicgstab; }
     void begin(DVec &x, DVec &b, const std::vector<double> &conv);
     bool started();
     void step();
     bool stepped();
+    void finish();
 
   private:
     bool check(const double *res, const double *res0, std::vector<double> &iconv);
@@ -124,15 +127,18 @@ class Krylov : public SolverBase {
     void solve_rbicgstab(DVec &x, DVec &b, const std::vector<double> &conv);
     void upload_iconv(const std::vector<double> &iconv);
     void step_body();
+    void step_tail();
     // per (out, in, in.zero, lane): a graph's kernels carry its lane's scratch
     std::map<std::tuple<const void *, const void *, bool, int>, MGraph> graphs_;
-    // step() as one graph per lane (the work vectors are fixed from setup on)
-    std::map<int, MGraph> step_graphs_;
+    // step() as one graph per (lane, tail, x): the work vectors are fixed from
+    // setup on; a tail updates x
+    std::map<std::tuple<int, bool, const void *>, MGraph> step_graphs_;
     bool capturing_ = false;  // recording step(): preconditioner runs inline
     // state of the merged BiCGStab solve between its steps
     struct Run {
         DVec *x = nullptr, *b = nullptr, *pa = nullptr, *sa = nullptr;
         std::vector<double> iconv, rho0, res;
+        bool tail = false;  // the rest of the last iteration is not launched yet
     } run_;
 };
 

@@ -122,3 +122,24 @@ def test_repeated_solves_equal(gpu):
     first = run_each(sys_)
     same(run_each(sys_), first)
     same(run_batch(gpu, sys_), first)
+
+
+@pytest.mark.parametrize("method", ["MergedPBiCGStab", "MergedBiCGStab"])
+def test_batch_stopped_at_max_iters(gpu, method):
+    """Systems that stop at max_iters before converging, beside one that
+    converges: the rest of each system's last iteration (its x update) still
+    runs, so every result equals its single solve bit for bit, on the first
+    call and once the iterations replay as graphs."""
+    specs = []
+    for i, (edge, nv, cap) in enumerate([(20, 4, 7), (16, 1, 5), (12, 2, 2000)]):
+        p = config3_params(method)
+        p["solver"]["max_iters"] = cap
+        if method == "MergedBiCGStab":
+            p = {"solver": p["solver"]}
+        specs.append((edge, nv, 40 + i, p))
+    sys_ = systems(gpu, specs)
+    want = run_each(sys_)
+    assert not want[0][1]["conv"].all() and want[0][1]["iters"] == 7
+    assert want[2][1]["conv"].all()
+    for _ in range(4):
+        same(run_batch(gpu, sys_), want)

@@ -261,20 +261,24 @@ def test_graph_replay_matches_direct_launches(gpu, smoother):
     assert l0 == l1
 
 
-@pytest.mark.parametrize("method,prec", [("MergedPBiCGStab", "Jacobi"),
-                                         ("PBiCGStab", "MultiGrid"),
-                                         ("MergedBiCGStab", None)])
-def test_step_graph_matches_direct_launches(gpu, oracle, method, prec):
-    """gpu_graph = 1 also records one BiCGStab iteration up to its residual as
-    a CUDA graph on its third call and replays it from the fourth. Over a
-    solve of many iterations the replayed form must give the direct launches'
-    solution, iterations and kernel count bit for bit, and match the oracle."""
+@pytest.mark.parametrize("method,prec,cap", [("MergedPBiCGStab", "Jacobi", 200),
+                                             ("MergedPBiCGStab", "Jacobi", 9),
+                                             ("PBiCGStab", "MultiGrid", 200),
+                                             ("MergedBiCGStab", None, 200),
+                                             ("MergedBiCGStab", None, 11)])
+def test_step_graph_matches_direct_launches(gpu, oracle, method, prec, cap):
+    """gpu_graph = 1 also records each BiCGStab iteration (the previous
+    iteration's x, r and p updates, then the iteration up to its residual) as
+    a CUDA graph on its third call and replays it from then on. Over a solve
+    of many iterations, converged or stopped at max_iters (cap), the replayed
+    form must give the direct launches' solution, iterations and kernel count
+    bit for bit, and match the oracle."""
     row, col, val = gpu.generate_cube(24, 24, 24)
     nv = 2
     b = np.random.default_rng(5).uniform(-1, 1, (len(row) - 1) * nv)
     out = []
     for graph in (0, 1):
-        params = {"solver": {"method": method, "max_iters": 200, "rel_tolerance": 1e-8,
+        params = {"solver": {"method": method, "max_iters": cap, "rel_tolerance": 1e-8,
                              "abs_tolerance": 0, "gpu_graph": graph}}
         if prec == "Jacobi":
             params["preconditioner"] = {"method": "Jacobi"}
@@ -287,10 +291,12 @@ def test_step_graph_matches_direct_launches(gpu, oracle, method, prec):
         out.append((x, st, gpu.kernel_launches() - k0))
     (x0, s0, l0), (x1, s1, l1) = out
     assert s0["iters"] == s1["iters"] and s0["iters"] >= 5
+    assert (s0["iters"] == cap) == (cap < 100)
     assert x0.tobytes() == x1.tobytes()
     assert l0 == l1
     xo, so, _ = oracle_solve(oracle, S, row, col, val, nv, params, b, 1)
     assert s1["iters"] == so["iters"]
+    assert s1["conv"].tolist() == so["conv"].tolist()
     assert x1.tobytes() == xo.tobytes()
 
 
