@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 
 #include "host_num.h"
 #include "ops.h"
@@ -90,6 +91,14 @@ static void read_scalars(const double *dev, double *host, int nv) {
     XG_CUDA(cudaStreamSynchronize(c.stream));
     std::memcpy(host, c.pinned, nv * sizeof(double));
 }
+
+// Posts nv device scalars to the current lane's pinned slots; take_scalars
+// reads them once the lane's stream has been synchronised.
+static void post_scalars(const double *dev, int nv) {
+    Ctx &c = ctx();
+    XG_CUDA(cudaMemcpyAsync(c.pinned, dev, nv * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+}
+static void take_scalars(double *host, int nv) { std::memcpy(host, ctx().pinned, nv * sizeof(double)); }
 
 // get_residual (solver.h:243-256) with the norm into res (host)
 template <typename F>
@@ -773,8 +782,9 @@ void Krylov::solve_pcg(DVec &x, DVec &b, const std::vector<double> &conv) {
     p.zero = z.zero;
     if (!z.zero) ops::convert<double, double>(p.p<double>(), z.p<double>(), p.elems(), s);
     ops::pcg_dots(n, r.p<double>(), z.p<double>(), SC, true, NV, s);
-    do {
-        ++st.iters;
+    // one iteration up to the copy of its residual; with gpu_graph (default)
+    // one graph per (lane, x.zero, x) through run_graphed
+    auto body = [&] {
         ops::pcg_ap(*A, p.p<double>(), Ap.p<double>(), SC, NV, s);
         Ap.zero = false;
         ops::pcg_xr(n, x.p<double>(), r.p<double>(), p.p<double>(), Ap.p<double>(), SC, x.zero,
@@ -784,7 +794,17 @@ void Krylov::solve_pcg(DVec &x, DVec &b, const std::vector<double> &conv) {
         apply_M(z, r);
         ops::pcg_dots(n, r.p<double>(), z.p<double>(), SC, false, NV, s);
         ops::pcg_p(n, p.p<double>(), z.p<double>(), SC, NV, s);
-        read_scalars(SC + k::SC_RES * k::SC_STRIDE, res.data(), NV);
+        post_scalars(SC + k::SC_RES * k::SC_STRIDE, NV);
+    };
+    do {
+        ++st.iters;
+        if (cfg.gpu_graph)
+            run_graphed(step_graph(std::make_tuple(ctx().lane, x.zero, x.p<const void>())), &x,
+                        body);
+        else
+            body();
+        XG_CUDA(cudaStreamSynchronize(s));
+        take_scalars(res.data(), NV);
         if (check(res.data(), rho0.data(), iconv)) return;
     } while (st.iters < cfg.max_iters);
     XG_CUDA(cudaStreamSynchronize(s));
@@ -877,13 +897,6 @@ void Krylov::solve(DVec &x, DVec &b, const std::vector<double> &conv) {
     XG_CUDA(cudaStreamSynchronize(S()));
 }
 
-// Posts nv device scalars to the current lane's pinned slots; take_scalars
-// reads them once the lane's stream has been synchronised.
-static void post_scalars(const double *dev, int nv) {
-    Ctx &c = ctx();
-    XG_CUDA(cudaMemcpyAsync(c.pinned, dev, nv * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-}
-static void take_scalars(double *host, int nv) { std::memcpy(host, ctx().pinned, nv * sizeof(double)); }
 
 // merged_bicgstab.inl:44-208 / merged_pbicgstab.inl:44-225
 void Krylov::begin(DVec &x, DVec &b, const std::vector<double> &conv) {
@@ -917,37 +930,25 @@ bool Krylov::started() {
     return check(run_.rho0.data(), run_.rho0.data(), run_.iconv);
 }
 
-// The previous iteration's tail (when its residual did not converge) and
-// this iteration up to its residual. With gpu_graph (default) these are
-// recorded as one CUDA graph per (lane, tail or not, x) on the third call
-// (the first two settle the preconditioner's graphs, flags and launch
-// shapes; the recording runs the preconditioner's kernels inline) and
-// replayed from then on: the same kernels and the same copy of the residual
-// to the lane's pinned slots, on the same buffers, in one launch. The work
-// vectors' flags are restored as the recording left them. A step that
-// cannot be captured runs directly.
-void Krylov::step() {
-    ++st.iters;
-    run_.pa = M ? &buf[6] : &buf[2];
-    run_.sa = M ? &buf[7] : &buf[4];
-    const bool tail = run_.tail;
-    run_.tail = false;
-    auto body = [&] {
-        if (tail) step_tail();
-        step_body();
-    };
-    if (!cfg.gpu_graph) {
-        body();
-        return;
-    }
-    const auto key = std::make_tuple(ctx().lane, tail, run_.x->p<const void>());
+// The step graph for key; past 32 keys (many solution vectors) the graphs
+// start over rather than keep one for each.
+MGraph &Krylov::step_graph(const std::tuple<int, bool, const void *> &key) {
     if (step_graphs_.size() >= 32 && !step_graphs_.count(key)) {
-        // many solution vectors: start over rather than keep a graph for each
         for (auto &kv : step_graphs_)
             if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
         step_graphs_.clear();
     }
-    MGraph &g = step_graphs_[key];
+    return step_graphs_[key];
+}
+
+// Runs body() directly on its first two calls for g (they settle the
+// preconditioner's graphs, flags and launch shapes), records it as a CUDA
+// graph on the third (the preconditioner's kernels inline) and replays it
+// from then on: the same kernels and copies on the same buffers in one
+// launch. The work vectors' flags, and x's when given (a body that writes
+// x), are restored as the recording left them. A body that cannot be
+// captured runs directly from then on.
+void Krylov::run_graphed(MGraph &g, DVec *x, const std::function<void()> &body) {
     if (g.exec) {
         XG_CUDA(cudaGraphLaunch(g.exec, S()));
         g_kernel_launches += g.launches;
@@ -955,7 +956,10 @@ void Krylov::step() {
             buf[i].zero = g.flags[i] & 1;
             buf[i].init = g.flags[i] & 2;
         }
-        if (tail) run_.x->zero = false;
+        if (x) {
+            x->zero = g.flags[buf.size()] & 1;
+            x->init = g.flags[buf.size()] & 2;
+        }
         return;
     }
     if (g.failed || g.calls++ < 2) {
@@ -988,10 +992,32 @@ void Krylov::step() {
     }
     cudaGraphDestroy(graph);
     g.launches = g_kernel_launches - l0;
-    g.flags.resize(buf.size());
-    for (size_t i = 0; i < buf.size(); ++i)
-        g.flags[i] = (uint8_t)((buf[i].zero ? 1 : 0) | (buf[i].init ? 2 : 0));
+    auto code = [](const DVec &v) { return (uint8_t)((v.zero ? 1 : 0) | (v.init ? 2 : 0)); };
+    g.flags.resize(buf.size() + 1);
+    for (size_t i = 0; i < buf.size(); ++i) g.flags[i] = code(buf[i]);
+    g.flags[buf.size()] = x ? code(*x) : 0;
     XG_CUDA(cudaGraphLaunch(g.exec, S()));
+}
+
+// The previous iteration's tail (when its residual did not converge) and
+// this iteration up to its residual; with gpu_graph (default) one graph per
+// (lane, tail or not, x) through run_graphed.
+void Krylov::step() {
+    ++st.iters;
+    run_.pa = M ? &buf[6] : &buf[2];
+    run_.sa = M ? &buf[7] : &buf[4];
+    const bool tail = run_.tail;
+    run_.tail = false;
+    auto body = [&] {
+        if (tail) step_tail();
+        step_body();
+    };
+    if (!cfg.gpu_graph) {
+        body();
+        return;
+    }
+    run_graphed(step_graph(std::make_tuple(ctx().lane, tail, run_.x->p<const void>())),
+                tail ? run_.x : nullptr, body);
 }
 
 void Krylov::step_body() {

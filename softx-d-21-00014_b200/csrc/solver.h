@@ -5,6 +5,7 @@
 // kernels that write the same values.
 #pragma once
 
+#include <functional>
 #include <map>
 #include <tuple>
 #include <memory>
@@ -128,10 +129,12 @@ class Krylov : public SolverBase {
     void upload_iconv(const std::vector<double> &iconv);
     void step_body();
     void step_tail();
+    MGraph &step_graph(const std::tuple<int, bool, const void *> &key);
+    void run_graphed(MGraph &g, DVec *x, const std::function<void()> &body);
     // per (out, in, in.zero, lane): a graph's kernels carry its lane's scratch
     std::map<std::tuple<const void *, const void *, bool, int>, MGraph> graphs_;
-    // step() as one graph per (lane, tail, x): the work vectors are fixed from
-    // setup on; a tail updates x
+    // iteration graphs: BiCGStab per (lane, tail, x), PCG per (lane, x.zero,
+    // x); the work vectors are fixed from setup on, x is the caller's
     std::map<std::tuple<int, bool, const void *>, MGraph> step_graphs_;
     bool capturing_ = false;  // recording step(): preconditioner runs inline
     // state of the merged BiCGStab solve between its steps
