@@ -837,8 +837,22 @@ void Krylov::solve_rbicgstab(DVec &x, DVec &b, const std::vector<double> &conv) 
     apply_M(z, r0);
     v_.zero = z.zero;
     if (!z.zero) ops::convert<double, double>(v_.p<double>(), z.p<double>(), v_.elems(), s);
-    do {
-        ++st.iters;
+    // group 2 of a non-converged iteration runs at the start of the next
+    // one, so that from the second iteration on the whole iteration up to
+    // the copy of its residual is one graph per (lane, x.zero, x) through
+    // run_graphed (gpu_graph, default)
+    auto group2 = [&] {
+        ops::rb_group2(n, x.p<double>(), v_.p<double>(), z.p<double>(), t_.p<double>(),
+                       s_.p<double>(), SC, rb_merged, x.zero, NV, s);
+        z.zero = v_.zero = false;
+        if (rb_merged) {
+            x.zero = false;
+            x.init = true;
+        }
+    };
+    bool tail = false;
+    auto body = [&] {
+        if (tail) group2();
         ops::spmv_dot_alpha(*A, v_.p<double>(), v.p<double>(), r0.p<double>(), SC, NV, s);
         v.zero = false;
         apply_M(s_, v);
@@ -854,7 +868,18 @@ void Krylov::solve_rbicgstab(DVec &x, DVec &b, const std::vector<double> &conv) 
             x.zero = false;
             x.init = true;
         }
-        read_scalars(SC + k::SC_RES * k::SC_STRIDE, res.data(), NV);
+        post_scalars(SC + k::SC_RES * k::SC_STRIDE, NV);
+    };
+    do {
+        ++st.iters;
+        if (cfg.gpu_graph && tail)
+            run_graphed(step_graph(std::make_tuple(ctx().lane, x.zero, x.p<const void>())), &x,
+                        body);
+        else
+            body();
+        tail = false;
+        XG_CUDA(cudaStreamSynchronize(s));
+        take_scalars(res.data(), NV);
         if (check(res.data(), rho0.data(), iconv)) {
             if (rb_merged) {
                 ops::rb_x(n, x.p<double>(), v_.p<double>(), t_.p<double>(), SC, x.zero, NV, s);
@@ -863,14 +888,9 @@ void Krylov::solve_rbicgstab(DVec &x, DVec &b, const std::vector<double> &conv) 
             }
             return;
         }
-        ops::rb_group2(n, x.p<double>(), v_.p<double>(), z.p<double>(), t_.p<double>(),
-                       s_.p<double>(), SC, rb_merged, x.zero, NV, s);
-        z.zero = v_.zero = false;
-        if (rb_merged) {
-            x.zero = false;
-            x.init = true;
-        }
+        tail = true;
     } while (st.iters < cfg.max_iters);
+    group2();
     XG_CUDA(cudaStreamSynchronize(s));
 }
 

@@ -133,8 +133,9 @@ class Krylov : public SolverBase {
     void run_graphed(MGraph &g, DVec *x, const std::function<void()> &body);
     // per (out, in, in.zero, lane): a graph's kernels carry its lane's scratch
     std::map<std::tuple<const void *, const void *, bool, int>, MGraph> graphs_;
-    // iteration graphs: BiCGStab per (lane, tail, x), PCG per (lane, x.zero,
-    // x); the work vectors are fixed from setup on, x is the caller's
+    // iteration graphs: BiCGStab per (lane, tail, x), PCG and RBiCGStab per
+    // (lane, x.zero, x); the work vectors are fixed from setup on, x is the
+    // caller's
     std::map<std::tuple<int, bool, const void *>, MGraph> step_graphs_;
     bool capturing_ = false;  // recording step(): preconditioner runs inline
     // state of the merged BiCGStab solve between its steps

@@ -267,12 +267,15 @@ def test_graph_replay_matches_direct_launches(gpu, smoother):
                                              ("MergedBiCGStab", None, 200),
                                              ("MergedBiCGStab", None, 11),
                                              ("PCG", "MultiGrid", 200),
-                                             ("PCG", None, 12)])
+                                             ("PCG", None, 12),
+                                             ("RBiCGStab", "MultiGrid", 200),
+                                             ("MergedRBiCGStab", "Jacobi", 200),
+                                             ("MergedRBiCGStab", "Jacobi", 10)])
 def test_step_graph_matches_direct_launches(gpu, oracle, method, prec, cap):
     """gpu_graph = 1 also records each BiCGStab iteration (the previous
     iteration's x, r and p updates, then the iteration up to its residual),
-    and each PCG iteration, as a CUDA graph on its third call and replays it
-    from then on. Over a solve
+    and each PCG or RBiCGStab iteration, as a CUDA graph on its third call
+    and replays it from then on. Over a solve
     of many iterations, converged or stopped at max_iters (cap), the replayed
     form must give the direct launches' solution, iterations and kernel count
     bit for bit, and match the oracle."""
