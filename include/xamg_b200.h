@@ -235,6 +235,11 @@ void *XAMG_b200_stream(void);
  * ranks to cores through XAMG_NUMACONF instead). */
 int XAMG_b200_set_device(int device);
 
+/* Architecture of the library's device code as the CUDA runtime reports it
+ * for a kernel of the library (cudaFuncGetAttributes): binary_version 100
+ * means sm_100 machine code (no counterpart in the reference). */
+int XAMG_b200_kernel_arch(int *binary_version, int *ptx_version);
+
 /* Device address of a vector's [size][nv] storage (no counterpart). */
 int XAMG_b200_vector_device_ptr(size_t vid, void **ptr);
 

@@ -87,6 +87,10 @@ static void core_range(uint64_t n, int ncores, int core, uint64_t &offset, uint6
 // ----------------------------------------------------------------------------
 // Reduction orders
 // ----------------------------------------------------------------------------
+// Element-wise loops over vector entries are independent (each entry is
+// computed by one thread from its own inputs), so threads change no result.
+#define OR_PAR _Pragma("omp parallel for schedule(static)")
+
 struct RedCfg {
     int mode = 0;    // 0: XAMG core-partitioned sequential, 1: B200 canonical
     int ncores = 1;  // XAMG cores of the single NUMA domain
@@ -111,8 +115,13 @@ static void canon_reduce(uint64_t n, int NV, int nred, Term term, T *out) {
     const uint64_t ntiles = (n + R - 1) / R;
     const uint64_t B = std::min<uint64_t>(ntiles, CANON_BMAX);
     std::vector<T> partial(B * NV * nred);
+    // blocks are independent until their partials are combined below, so
+    // they run on the host threads without changing any sum
+#pragma omp parallel
+    {
     std::vector<T> acc(CANON_THREADS * nred);
     std::vector<T> v(nred);
+#pragma omp for schedule(static)
     for (uint64_t b = 0; b < B; ++b) {
         std::fill(acc.begin(), acc.end(), T(0));
         for (int t = 0; t < CANON_THREADS; ++t) {
@@ -144,6 +153,7 @@ static void canon_reduce(uint64_t n, int NV, int nred, Term term, T *out) {
                 partial[(b * NV + k) * nred + r] = s;
             }
     }
+    }
     for (int k = 0; k < NV; ++k)
         for (int r = 0; r < nred; ++r) {
             T lane[32], tmp[32];
@@ -167,8 +177,10 @@ template <typename T, typename Term>
 static void xamg_reduce(uint64_t n, int NV, int nred, Term term, T *out) {
     const int ncores = std::max(1, g_red.ncores);
     std::vector<T> part(ncores * NV * nred, T(0));
-    std::vector<T> v(nred);
+    // each core's partial is summed on its own, as XAMG's ranks do
+#pragma omp parallel for schedule(static, 1)
     for (int c = 0; c < ncores; ++c) {
+        std::vector<T> v(nred);
         uint64_t off, sz;
         core_range(n, ncores, c, off, sz);
         T *p = &part[c * NV * nred];
@@ -273,8 +285,10 @@ void set_const_v(Vec &x, const Vec &val, bool force) {
     const T *vp = val.p<T>();
     const int NV = x.nv;
     if (val.size == 1 && val.nv == 1) {
+        OR_PAR
         for (uint64_t i = 0; i < x.size * NV; ++i) xp[i] = vp[0];
     } else {
+        OR_PAR
         for (uint64_t i = 0; i < x.size * NV; i += NV)
             for (int k = 0; k < NV; ++k) xp[i + k] = vp[k];
     }
@@ -322,8 +336,10 @@ void ax_y(const Vec &a, const Vec &x, Vec &y) {
     T *yp = y.p<T>();
     const T *ap = a.p<T>();
     if (a.nv == 1) {
+        OR_PAR
         for (uint64_t i = 0; i < NV * y.size; ++i) yp[i] = ap[0] * xp[i];
     } else {
+        OR_PAR
         for (uint64_t i = 0; i < NV * y.size; i += NV)
             for (int k = 0; k < NV; ++k) yp[i + k] = ap[k] * xp[i + k];
     }
@@ -355,8 +371,10 @@ void axpby(const Vec &a, const Vec &x, const Vec &b, Vec &y) {
     const T *ap = a.p<T>();
     const T *bp = b.p<T>();
     if (a.nv == 1) {
+        OR_PAR
         for (uint64_t i = 0; i < NV * y.size; ++i) yp[i] = ap[0] * xp[i] + bp[0] * yp[i];
     } else {
+        OR_PAR
         for (uint64_t i = 0; i < NV * y.size; i += NV)
             for (int k = 0; k < NV; ++k) yp[i + k] = ap[k] * xp[i + k] + bp[k] * yp[i + k];
     }
@@ -393,16 +411,20 @@ void scal(const Vec &x, Vec &y) {
     T *yp = y.p<T>();
     if (x.nv == 1) {
         if (x.size == 1) {
+            OR_PAR
             for (uint64_t i = 0; i < NV * y.size; ++i) yp[i] *= xp[0];
         } else {
+            OR_PAR
             for (uint64_t i = 0; i < y.size; ++i)
                 for (int k = 0; k < NV; ++k) yp[i * NV + k] *= xp[i];
         }
     } else {
         if (x.size == 1) {
+            OR_PAR
             for (uint64_t i = 0; i < NV * y.size; i += NV)
                 for (int k = 0; k < NV; ++k) yp[i + k] *= xp[k];
         } else {
+            OR_PAR
             for (uint64_t i = 0; i < NV * y.size; ++i) yp[i] *= xp[i];
         }
     }
@@ -423,6 +445,7 @@ void copy(const Vec &x, Vec &y) {
     }
     const T *xp = x.p<T>();
     T *yp = y.p<T>();
+    OR_PAR
     for (uint64_t i = 0; i < (uint64_t)x.nv * x.size; ++i) yp[i] = xp[i];
     y.init = true;
     y.zero = false;
@@ -476,9 +499,11 @@ void axpby_z(const Vec &a, const Vec &x, const Vec &b, const Vec &y, Vec &z) {
     const T *ap = a.p<T>();
     const T *bp = b.p<T>();
     if (a.nv == 1) {
+        OR_PAR
         for (uint64_t i = 0; i < NV * z.size; i += NV)
             for (int k = 0; k < NV; ++k) zp[i + k] = ap[0] * xp[i + k] + bp[0] * yp[i + k];
     } else {
+        OR_PAR
         for (uint64_t i = 0; i < NV * z.size; i += NV)
             for (int k = 0; k < NV; ++k) zp[i + k] = ap[k] * xp[i + k] + bp[k] * yp[i + k];
     }
@@ -513,10 +538,12 @@ void axpbypcz(const Vec &a, const Vec &x, const Vec &b, const Vec &y, const Vec 
     const T *bp = b.p<T>();
     const T *cp = c.p<T>();
     if (a.nv == 1) {
+        OR_PAR
         for (uint64_t i = 0; i < NV * z.size; i += NV)
             for (int k = 0; k < NV; ++k)
                 zp[i + k] = ap[0] * xp[i + k] + bp[0] * yp[i + k] + cp[0] * zp[i + k];
     } else {
+        OR_PAR
         for (uint64_t i = 0; i < NV * z.size; i += NV)
             for (int k = 0; k < NV; ++k)
                 zp[i + k] = ap[k] * xp[i + k] + bp[k] * yp[i + k] + cp[k] * zp[i + k];
@@ -535,6 +562,7 @@ void xdivy_z(const Vec &x, const Vec &y, Vec &z) {
     const T *xp = x.p<T>();
     const T *yp = y.p<T>();
     T *zp = z.p<T>();
+    OR_PAR
     for (uint64_t i = 0; i < (uint64_t)x.nv * x.size; ++i) zp[i] = xp[i] / yp[i];
     z.init = true;
     z.zero = false;
@@ -551,6 +579,7 @@ void merged_bicgstab_group1(Vec &r0, Vec &b, Vec &p, Vec &r, Vec &rho0) {
     T *pp = p.p<T>();
     T *rp = r.p<T>();
     // elementwise part first; the sums do not feed back into it
+    OR_PAR
     for (uint64_t i = 0; i < NV * r0.size; ++i) {
         r0p[i] = bp[i] - r0p[i];
         pp[i] = r0p[i];
@@ -601,6 +630,7 @@ void merged_bicgstab_group4(Vec &s, Vec &t, Vec &r0, Vec &r, const Vec &omega, V
     const T *r0p = r0.p<T>();
     T *rp = r.p<T>();
     const T *op = omega.p<T>();
+    OR_PAR
     for (uint64_t i = 0; i < NV * s.size; i += NV)
         for (int k = 0; k < NV; ++k) rp[i + k] = sp[i + k] - op[k] * tp[i + k];
     reduce<T>(s.size, NV, 1,
@@ -634,6 +664,7 @@ void merged_bicgstab_group5(Vec &x, Vec &p, Vec &s, Vec &r, Vec &v, const Vec &a
     const T *op = omega.p<T>();
     std::vector<T> val(NV);
     for (int k = 0; k < NV; ++k) val[k] = bp[k] * op[k];
+    OR_PAR
     for (uint64_t i = 0; i < NV * s.size; i += NV)
         for (int k = 0; k < NV; ++k) {
             xp[i + k] += ac[k] * pp[i + k] + oc[k] * sp[i + k];
@@ -656,6 +687,7 @@ void merged_rbicgstab_group1(Vec &r, Vec &v, Vec &t, Vec &r0, const Vec &alpha, 
     const int NV = r.nv;
     T *rp = r.p<T>();
     const T *vp = v.p<T>(), *tp = t.p<T>(), *r0p = r0.p<T>(), *ap = alpha.p<T>();
+    OR_PAR
     for (uint64_t i = 0; i < NV * r.size; i += NV)
         for (int k = 0; k < NV; ++k) rp[i + k] = rp[i + k] - ap[k] * vp[i + k];
     std::vector<T> out(4 * NV);
@@ -696,6 +728,7 @@ void merged_rbicgstab_group2(Vec &x, Vec &v_, Vec &t_, Vec &z, Vec &s, const Vec
     const T *tp = t_.p<T>(), *sp = s.p<T>();
     const T *ac = alpha_conv.p<T>(), *oc = omega_conv.p<T>(), *om = omega.p<T>(),
             *be = beta.p<T>();
+    OR_PAR
     for (uint64_t i = 0; i < NV * x.size; i += NV)
         for (int k = 0; k < NV; ++k) {
             xp[i + k] += ac[k] * vp[i + k] + oc[k] * tp[i + k];
@@ -719,12 +752,14 @@ void merged_jacobi(Vec &x, const Vec &b, const Vec &inv_diag, Vec &r, const Vec 
     const T *rp = r.p<T>();
     const T *wp = relax.p<T>();
     if (x.zero && r.zero) {
+        OR_PAR
         for (uint64_t i = 0; i < x.size; i++)
             for (int k = 0; k < NV; ++k) xp[i * NV + k] = wp[k] * dp[i] * bp[i * NV + k];
     } else {
         if (x.zero) forced_set_const<T>(x, 0.0);
         if (r.zero) forced_set_const<T>(r, 0.0);
         rp = r.p<T>();
+        OR_PAR
         for (uint64_t i = 0; i < x.size; i++)
             for (int k = 0; k < NV; ++k)
                 xp[i * NV + k] += wp[k] * dp[i] * (bp[i * NV + k] - rp[i * NV + k]);
@@ -1042,6 +1077,7 @@ void dense_Ax_y(const std::vector<T> &a, uint64_t n, const Vec &x, Vec &y) {
     const int NV = y.nv;
     const T *xp = x.p<T>();
     T *yp = y.p<T>();
+    OR_PAR
     for (uint64_t i = 0; i < n; ++i) {
         for (int k = 0; k < NV; ++k) yp[i * NV + k] = 0.0;
         for (uint64_t j = 0; j < n; ++j)
@@ -1383,8 +1419,11 @@ static void sgs(Solver &S, const Vec &b, Vec &x, Vec &t, const Vec &relax) {
     const T *tp = t.p<T>();
     const T *dp = S.id.p<T>();
     const T *wp = relax.p<T>();
-    std::vector<T> sum(NV), coeff(NV);
+    // a core block reads and writes only its own rows of x (the off-core
+    // terms are in t), so the blocks run on the host threads independently
+#pragma omp parallel for schedule(static)
     for (int c = 0; c < L.ncores; ++c) {
+        std::vector<T> sum(NV), coeff(NV);
         const Csr &m = L.diag[c];
         if (m.empty()) {
             continue;
@@ -1528,10 +1567,13 @@ static void convert_vec(const Vec &src, Vec &dst) {
         return;
     }
     const uint64_t m = (uint64_t)src.size * src.nv;
-    if (src.f32 && !dst.f32)
+    if (src.f32 && !dst.f32) {
+        OR_PAR
         for (uint64_t i = 0; i < m; ++i) dst.d[i] = (double)src.f[i];
-    else if (!src.f32 && dst.f32)
+    } else if (!src.f32 && dst.f32) {
+        OR_PAR
         for (uint64_t i = 0; i < m; ++i) dst.f[i] = (float)src.d[i];
+    }
     else if (src.f32)
         dst.f = src.f;
     else

@@ -682,6 +682,21 @@ int XAMG_b200_last_error(char *buf, size_t len) {
     return (int)g_last_error.size();
 }
 
+// Never launched: its attributes tell which architecture the library's
+// device code was compiled for.
+static __global__ void k_arch_query() {}
+
+int XAMG_b200_kernel_arch(int *binary_version, int *ptx_version) {
+    return guarded([&] {
+        XG_REQUIRE(binary_version && ptx_version, XAMG_ERR_INVALID_ARG, "null pointer");
+        ctx();
+        cudaFuncAttributes a;
+        XG_CUDA(cudaFuncGetAttributes(&a, k_arch_query));
+        *binary_version = a.binaryVersion;
+        *ptx_version = a.ptxVersion;
+    });
+}
+
 int XAMG_b200_build_info(char *buf, size_t len) {
     const char *s = "sm_100a";
     if (buf && len) {

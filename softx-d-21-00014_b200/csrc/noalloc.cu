@@ -13,9 +13,13 @@
 // that loads this library, for as long as the process runs. Host code never
 // passes the array's name to a kernel (in host code that name is only a
 // stand-in); the device address is looked up once per device with
-// cudaGetSymbolAddress, with that device current, on the first call made on
-// that device. That first call should therefore come before any stream
-// capture. Inputs and the output are the caller's device arrays.
+// cudaGetSymbolAddress, with that device current. XAMG_init does this for the
+// library's device, and also loads the kernels this entry point launches, so
+// that under CUDA's lazy module loading no call on that device loads code or
+// maps the array. On any other device the first call does the lookup and the
+// loading itself (which may allocate and synchronise), so make that first call
+// before any stream capture and outside the region that must not allocate.
+// Inputs and the output are the caller's device arrays.
 //
 // Limits: nv must be 1, 2, 4, 8, 16 or 32; the array holds 1184 x 32 partial
 // sums (303,104 bytes) plus the counter, enough for every row count since the
@@ -52,6 +56,12 @@ int scratch_for_current_device(double **out) {
 }
 
 template <int NV>
+cudaError_t load_dot_kernel() {
+    cudaFuncAttributes a;
+    return cudaFuncGetAttributes(&a, k::k_rows<double, NV, 1, k::EDot<double, NV>>);
+}
+
+template <int NV>
 int launch_dot(uint64_t n, const double *x, const double *y, double *out, double *scratch,
                cudaStream_t s) {
     unsigned *ticket = (unsigned *)(scratch + NOALLOC_PARTIALS);
@@ -63,6 +73,22 @@ int launch_dot(uint64_t n, const double *x, const double *y, double *out, double
 }
 
 }  // namespace
+
+// Called by the library's initialisation with its device current: resolves
+// the array's address and loads every kernel the entry point can launch.
+namespace ops {
+int noalloc_prepare_current_device() {
+    double *p = nullptr;
+    int rc = scratch_for_current_device(&p);
+    if (rc != XAMG_OK) return rc;
+    const cudaError_t e[] = {load_dot_kernel<1>(), load_dot_kernel<2>(), load_dot_kernel<4>(),
+                             load_dot_kernel<8>(), load_dot_kernel<16>(), load_dot_kernel<32>()};
+    for (cudaError_t x : e)
+        if (x != cudaSuccess) return XAMG_ERR_CUDA;
+    return XAMG_OK;
+}
+}  // namespace ops
+
 }  // namespace xg
 
 extern "C" int XAMG_b200_dot_noalloc(uint64_t n, int nv, const double *x, const double *y,

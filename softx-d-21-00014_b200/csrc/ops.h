@@ -14,6 +14,10 @@ namespace ops {
 // Launches a wait that must run out after limit_ns (raises the timeout flag).
 void wait_selftest(uint64_t limit_ns, cudaStream_t s);
 
+// Resolves the fixed scratch array of XAMG_b200_dot_noalloc and loads its
+// kernels on the current device (csrc/noalloc.cu); returns an XAMG status.
+int noalloc_prepare_current_device();
+
 template <typename F>
 void spmv(const DCsr &A, const F *x, F *y, int nv, bool axpy, cudaStream_t s);
 

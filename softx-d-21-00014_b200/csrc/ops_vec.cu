@@ -60,6 +60,9 @@ void Ctx::init() {
     XG_CUDA(cudaGetDevice(&device));
     XG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     lane_create(stream, red_part, red_ticket, red_out, pinned);
+    const int rc = ops::noalloc_prepare_current_device();
+    if (rc != XAMG_OK)
+        throw Error(rc, "cannot resolve the scratch array of XAMG_b200_dot_noalloc");
     lane = 0;
     ready = true;
 }

@@ -733,6 +733,7 @@ void Krylov::apply_M(DVec &out, DVec &in) {
         run_M(out, in);
         return;
     }
+    const bool in_zero = in.zero, in_init = in.init;
     XG_CUDA(cudaStreamSynchronize(S()));
     XG_CUDA(cudaStreamBeginCapture(S(), cudaStreamCaptureModeThreadLocal));
     const uint64_t l0 = g_kernel_launches;
@@ -746,12 +747,18 @@ void Krylov::apply_M(DVec &out, DVec &in) {
     const cudaError_t e = cudaStreamEndCapture(S(), &graph);
     if (!ok || e != cudaSuccess || !graph ||
         cudaGraphInstantiate(&g.exec, graph, 0) != cudaSuccess) {
-        // nothing ran during the capture: run directly from now on
+        // nothing ran during the capture: run directly from now on, from the
+        // flags the recording started with (it zero-flagged out, and may have
+        // cleared that flag as if its kernels had run)
         cudaGetLastError();
         if (graph) cudaGraphDestroy(graph);
         g.exec = nullptr;
         g.failed = true;
         g_kernel_launches = l0;
+        out.zero = true;
+        out.init = true;
+        in.zero = in_zero;
+        in.init = in_init;
         run_M(out, in);
         return;
     }
@@ -986,6 +993,28 @@ void Krylov::run_graphed(MGraph &g, DVec *x, const std::function<void()> &body) 
         body();
         return;
     }
+    auto code = [](const DVec &v) { return (uint8_t)((v.zero ? 1 : 0) | (v.init ? 2 : 0)); };
+    auto snapshot = [&](std::vector<uint8_t> &f) {
+        f.resize(buf.size() + 1);
+        for (size_t i = 0; i < buf.size(); ++i) f[i] = code(buf[i]);
+        f[buf.size()] = x ? code(*x) : 0;
+    };
+    auto restore = [&](const std::vector<uint8_t> &f) {
+        for (size_t i = 0; i < buf.size(); ++i) {
+            buf[i].zero = f[i] & 1;
+            buf[i].init = f[i] & 2;
+        }
+        if (x) {
+            x->zero = f[buf.size()] & 1;
+            x->init = f[buf.size()] & 2;
+        }
+    };
+    // The recording changes the host-side flags (x.zero, the work vectors'
+    // zero/init) as if the body had run. When the capture fails, the direct
+    // run below must start from the flags the body was called with, or its
+    // kernels would treat a zero-flagged x as holding values.
+    std::vector<uint8_t> before;
+    snapshot(before);
     XG_CUDA(cudaStreamSynchronize(S()));
     XG_CUDA(cudaStreamBeginCapture(S(), cudaStreamCaptureModeThreadLocal));
     const uint64_t l0 = g_kernel_launches;
@@ -1007,15 +1036,13 @@ void Krylov::run_graphed(MGraph &g, DVec *x, const std::function<void()> &body) 
         g.exec = nullptr;
         g.failed = true;
         g_kernel_launches = l0;
+        restore(before);
         body();
         return;
     }
     cudaGraphDestroy(graph);
     g.launches = g_kernel_launches - l0;
-    auto code = [](const DVec &v) { return (uint8_t)((v.zero ? 1 : 0) | (v.init ? 2 : 0)); };
-    g.flags.resize(buf.size() + 1);
-    for (size_t i = 0; i < buf.size(); ++i) g.flags[i] = code(buf[i]);
-    g.flags[buf.size()] = x ? code(*x) : 0;
+    snapshot(g.flags);
     XG_CUDA(cudaGraphLaunch(g.exec, S()));
 }
 

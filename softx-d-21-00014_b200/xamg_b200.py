@@ -55,6 +55,7 @@ EXT_SYMBOLS = [
     "XAMG_b200_solver_hierarchy_export", "XAMG_b200_vector_device_ptr",
     "XAMG_b200_solver_level_csr", "XAMG_b200_kernel_launches", "XAMG_b200_stream",
     "XAMG_b200_set_device", "XAMG_b200_dot_noalloc", "XAMG_b200_wait_selftest",
+    "XAMG_b200_kernel_arch",
     "XAMG_b200_solver_level_spmv", "XAMG_b200_read_system_size", "XAMG_b200_read_system",
     "XAMG_b200_write_system", "XAMG_b200_solver_hierarchy_save",
     "XAMG_b200_matrix_hierarchy_load", "XAMG_b200_gemm_bf16", "XAMG_b200_mlp_create",
@@ -175,6 +176,7 @@ def lib():
         "XAMG_b200_stream": (vp, []),
         "XAMG_b200_set_device": (C.c_int, [C.c_int]),
         "XAMG_b200_wait_selftest": (C.c_int, [C.c_double, C.POINTER(C.c_int)]),
+        "XAMG_b200_kernel_arch": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "XAMG_b200_solver_level_spmv": (C.c_int, [C.c_size_t, C.c_int, C.c_int, vp, vp, C.c_int,
                                                   C.c_int, vp]),
         "XAMG_b200_read_system_size": (C.c_int, [C.c_char_p, C.POINTER(C.c_uint32),

@@ -247,3 +247,95 @@ class System:
         L.or_sys_level_matrix(self.h, level, which, row.ctypes.data, col.ctypes.data,
                               val.ctypes.data, C.byref(f32), C.byref(nr), C.byref(nc))
         return row, col, val, nc.value
+
+
+# ---------------------------------------------------------------------------
+# Inputs of the CPU arm (oracle/liboracle_setup.so): the seeded generators and
+# the host multigrid setup compiled from the library's host-only sources, so
+# that a process that must not load the CUDA library gets the same matrix and
+# hierarchy bit for bit.
+# ---------------------------------------------------------------------------
+SETUP_LIB_PATH = os.path.join(ORACLE_DIR, "liboracle_setup.so")
+_setup = None
+
+# XAMG's MultiGrid family defaults (xamg_params_details.h:194-235) for the
+# keys the host setup reads, plus the library's seed key.
+MG_DEFAULTS = {"mg_strength_threshold": 0.5, "mg_max_row_sum": 0.9, "mg_max_levels": 25,
+               "mg_coarse_matrix_size": 100, "mg_trunc_factor": 0.25, "mg_Pmax_elements": 4,
+               "gpu_seed": 0}
+
+
+def setup_lib():
+    global _setup
+    if _setup is None:
+        if not os.path.exists(SETUP_LIB_PATH):
+            build()
+        L = C.CDLL(SETUP_LIB_PATH)
+        L.XAMG_b200_generate_diffusion.restype = C.c_int64
+        L.XAMG_b200_generate_diffusion.argtypes = [C.c_int] + [C.c_uint64] * 3 + [
+            C.c_double, C.c_double, C.c_uint64, u32p, u32p, f64p]
+        L.XAMG_b200_generate_cube.restype = C.c_int64
+        L.XAMG_b200_generate_cube.argtypes = [C.c_uint64] * 3 + [u32p, u32p, f64p]
+        L.os_hier_build.restype = C.c_void_p
+        L.os_hier_build.argtypes = [C.c_uint64, C.c_uint64, u32p, u32p, f64p, C.c_float,
+                                    C.c_float, C.c_int, C.c_int, C.c_float, C.c_int, C.c_int]
+        L.os_hier_free.argtypes = [C.c_void_p]
+        L.os_hier_levels.restype = C.c_int
+        L.os_hier_levels.argtypes = [C.c_void_p]
+        L.os_hier_level.argtypes = [C.c_void_p, C.c_int, C.c_int] + [C.POINTER(C.c_uint64)] * 3 + [
+            C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        _setup = L
+    return _setup
+
+
+def setup_generate_diffusion(stencil, nx, ny, nz, sigma, az, seed):
+    """The library's seeded diffusion generator (7- or 27-point)."""
+    n = nx * ny * nz
+    row = np.zeros(n + 1, np.uint32)
+    col = np.zeros(stencil * n, np.uint32)
+    val = np.zeros(stencil * n, np.float64)
+    nnz = setup_lib().XAMG_b200_generate_diffusion(stencil, nx, ny, nz, sigma, az, seed, row, col,
+                                                   val)
+    assert nnz >= 0
+    return row, col[:nnz].copy(), val[:nnz].copy()
+
+
+def setup_hierarchy(row, col, val, mg_params):
+    """The hierarchy the library's host setup builds for a MultiGrid list
+    `mg_params` (XAMG defaults for missing keys): a list of dicts
+    {A: (row, col, val), P: (row, col, val, ncols) or None, min_eig, max_eig},
+    as the library's solver hierarchy export gives it."""
+    L = setup_lib()
+    p = dict(MG_DEFAULTS)
+    p.update({k: v for k, v in mg_params.items() if k in MG_DEFAULTS})
+    n = len(row) - 1
+    h = L.os_hier_build(n, len(col), np.ascontiguousarray(row, np.uint32),
+                        np.ascontiguousarray(col, np.uint32), np.ascontiguousarray(val, np.float64),
+                        p["mg_strength_threshold"], p["mg_max_row_sum"], int(p["mg_max_levels"]),
+                        int(p["mg_coarse_matrix_size"]), p["mg_trunc_factor"],
+                        int(p["mg_Pmax_elements"]), int(p["gpu_seed"]))
+    try:
+        out = []
+        nl = L.os_hier_levels(h)
+        for lev in range(nl):
+            mats = []
+            for which in (0, 1):
+                nr, nc, nz = C.c_uint64(), C.c_uint64(), C.c_uint64()
+                mn, mx = C.c_double(), C.c_double()
+                L.os_hier_level(h, lev, which, C.byref(nr), C.byref(nc), C.byref(nz), None, None,
+                                None, C.byref(mn), C.byref(mx))
+                if nr.value == 0:
+                    mats.append(None)
+                    continue
+                r = np.zeros(nr.value + 1, np.uint32)
+                c = np.zeros(nz.value, np.uint32)
+                v = np.zeros(nz.value, np.float64)
+                L.os_hier_level(h, lev, which, C.byref(nr), C.byref(nc), C.byref(nz),
+                                r.ctypes.data, c.ctypes.data, v.ctypes.data, C.byref(mn),
+                                C.byref(mx))
+                mats.append((r, c, v, nc.value))
+            out.append(dict(A=mats[0][:3], P=mats[1] if lev + 1 < nl else None,
+                            min_eig=mn.value, max_eig=mx.value))
+        return out
+    finally:
+        L.os_hier_free(h)

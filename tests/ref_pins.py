@@ -7,12 +7,13 @@ import subprocess
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libxamg_ref.so")
-REF_SRC = "/root/reference/src"
 
 
 def load():
-    if not os.path.exists(REF_LIB) and os.path.isdir(REF_SRC):
-        subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"])
+    """The pins library, built on first use where the reference sources are
+    present (oracle/Makefile's XAMG_REF_SRC); None where they are not."""
+    if not os.path.exists(REF_LIB):
+        subprocess.call(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"])
     if not os.path.exists(REF_LIB):
         return None
     L = C.CDLL(REF_LIB)

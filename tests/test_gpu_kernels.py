@@ -184,3 +184,11 @@ def test_spmv_dot_fused(gpu, oracle, nv):
         assert dot.tobytes() == oracle.dot(v, z, nv).tobytes()
     finally:
         oracle.set_reduction(0)
+
+
+def test_kernels_are_sm100_machine_code(gpu):
+    """The CUDA runtime reports the library's kernels as sm_100 machine code."""
+    import ctypes as C
+    b, p = C.c_int(), C.c_int()
+    gpu.call("XAMG_b200_kernel_arch", C.byref(b), C.byref(p))
+    assert b.value == 100, (b.value, p.value)

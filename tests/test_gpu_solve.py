@@ -356,3 +356,50 @@ def test_autotuned_spmv_same_results(gpu, stencil, edge, nv, f32):
         assert (codes.any()) == bool(tune)
     assert out[0][0].tobytes() == out[1][0].tobytes()
     assert out[0][1]["iters"] == out[1][1]["iters"]
+
+
+@pytest.mark.parametrize("method", ["PCG", "MergedRBiCGStab"])
+def test_graph_fallback_keeps_zero_flag(gpu, method):
+    """A preconditioner that reads back its residual (Jacobi with
+    convergence_check) cannot be recorded into an iteration graph. The
+    recording attempt changes the host-side flags as if the iteration had
+    run; the direct run that follows must start from the flags it was called
+    with. Each solve writes into a fresh, zero-flagged x placed at the address
+    of the previous one (so its memory holds the previous solution): the
+    iteration graph key (lane, x zero, x) repeats, and the third solve is the
+    one whose recording fails. Every solve must equal the same solve without
+    graphs bit for bit."""
+    row, col, val = gpu.generate_diffusion(7, 16, 15, 14, 1.0, 1.0, 11)
+    n, nv = len(row) - 1, 2
+    M = gpu.Matrix(row, col, val)
+    B = gpu.Vector(n, nv, M.part)
+    b = np.random.default_rng(12).uniform(-1, 1, n * nv)
+    B.upload(b)
+    results = {}
+    for graph in (0, 1):
+        params = {"solver": {"method": method, "max_iters": 200, "rel_tolerance": 1e-8,
+                             "abs_tolerance": 0, "gpu_graph": graph},
+                  "preconditioner": {"method": "Jacobi", "max_iters": 2,
+                                     "convergence_check": 1, "rel_tolerance": 1e-12,
+                                     "abs_tolerance": 0}}
+        P = gpu.Params(params)
+        X = gpu.Vector(n, nv, M.part)
+        S = gpu.Solver(M, P, X, B)
+        addr, out = None, []
+        for i in range(4):
+            if i:
+                # a fresh vector where the last one was: zero-flagged, its
+                # memory still holding the previous solution
+                gpu.call("XAMG_vector_destroy", X.h)
+                X = gpu.Vector(n, nv, M.part)
+                assert X.device_ptr() == addr, "allocator did not reuse the address"
+            addr = X.device_ptr()
+            gpu.call("XAMG_solver_solve2", nv, X.h, B.h, S.h)
+            out.append((X.download(), S.stats()["iters"]))
+        results[graph] = out
+        gpu.call("XAMG_vector_destroy", X.h)
+    for (x0, i0), (x1, i1) in zip(results[0], results[1]):
+        assert i0 == i1
+        assert x0.tobytes() == x1.tobytes()
+    r = true_rel_res(row, col, val, results[1][-1][0], b, nv)
+    assert r.max() < 1e-7

@@ -40,3 +40,24 @@ def test_dot_noalloc_rejects_unsupported_nv(gpu):
     out = torch.zeros(3, dtype=torch.float64, device="cuda")
     rc = gpu.lib().XAMG_b200_dot_noalloc(10, 3, x.data_ptr(), x.data_ptr(), out.data_ptr(), None)
     assert rc == -2
+
+
+def test_dot_noalloc_allocates_nothing(gpu):
+    """XAMG_init resolved the array and loaded the entry point's kernels, so
+    calls on the library's device (every supported nv, repeated) leave the
+    device's free memory exactly as it was."""
+    import torch
+    n = 50000
+    x = torch.ones(n * 32, dtype=torch.float64, device="cuda")
+    out = torch.zeros(32, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(2):
+        for nv in (1, 2, 4, 8, 16, 32):
+            gpu.call("XAMG_b200_dot_noalloc", n, nv, x.data_ptr(), x.data_ptr(),
+                     out.data_ptr(), stream)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    assert out.cpu().numpy().tolist() == [float(n)] * 32
