@@ -16,10 +16,13 @@ upload b, solve, download x. Under torchrun every rank solves its own
 right-hand-side block on its own GPU (weak scaling, no data-path
 collective); times are the maximum over ranks.
 
---impl reference times the CPU oracle (the restatement of XAMG's FP64 CPU
-solve, its SpMV rows threaded over the host cores; the reference's own build
-needs MPI, hypre, argsparser and yaml-cpp) on a bounded sample of the same
-solve.
+--impl reference times the reference's own solve phase (XAMG's C API built
+from the reference sources into oracle/_ref with single-process stand-ins for
+MPI, argsparser and hypre: one rank, one core) on the same workload, alone in
+its process: inputs and hierarchy from oracle/liboracle_setup.so, then whole
+solves to the tolerance, one per step. The reference's MPI+shm parallel build
+cannot run here (no MPI); cpu_baseline of the GPU arm times the oracle port
+on all host threads beside it.
 """
 import argparse
 import json
@@ -231,7 +234,7 @@ def run_ours(args, w):
         with ClockSampler(local) as cs:
             ms, launches, _ = timed(S, args.steps)
         res[name] = dict(ms=ms, launches=launches, iters=st["iters"], conv=st["conv"].tolist(),
-                         rel_res=st["rel_res"].tolist(), clocks=cs.summary())
+                         rel_res=st["rel_res"].tolist(), clocks=cs.summary(), x=xv.download())
     S = solvers[chosen]
     ms_e2e, _, xh = timed(S, args.steps, e2e=True)
     # true residual of the chosen solve
@@ -244,6 +247,9 @@ def run_ours(args, w):
     # multigrid hierarchy (Jacobi-preconditioned configuration 1) has only A
     rf = roofline(X, torch, stream, S, n, nv, args, which=3 if w["smoother"] else 0)
     rf64 = roofline(X, torch, stream, S, n, nv, args, which=0)
+    # the plain FP64 method's level-0 SpMV (XAMG's narrowing, FP64 values)
+    rf_plain = roofline(X, torch, stream, solvers["fp64"], n, nv, args,
+                        which=3 if w["smoother"] else 0)
 
     total_rhs = args.steps * nv * ws
     out = {
@@ -257,10 +263,7 @@ def run_ours(args, w):
                   (f" (bf16 values on the {w['bf16_levels']} finest levels)"
                    if w.get("bf16_levels") else "")) if chosen == "chosen" else "f64",
         "data": "synthetic",
-        "config": {"workload": w["desc"], "rows": n, "nnz": int(len(col)), "nv": nv,
-                   "rhs_per_gpu_per_step": nv, "tolerance": 1e-8,
-                   "l2": "inputs larger than L2 (matrix > 126 MB)" if len(col) * 12 > 126e6
-                   else "L2-resident inputs (no flush)"},
+        "config": config_of(w, n, len(col)),
         "iters": {k: v["iters"] for k, v in res.items()},
         "plain_fp64_ms_per_rhs": res["fp64"]["ms"] / total_rhs * ws,
         "chosen_vs_fp64_speedup": res["fp64"]["ms"] / res[chosen]["ms"],
@@ -270,12 +273,16 @@ def run_ours(args, w):
         "gpu_launches": int(res[chosen]["launches"]),
         "roofline": rf,
         "roofline_krylov_spmv": rf64,
+        "roofline_plain_spmv": rf_plain,
         "clocks": res[chosen]["clocks"],
         "setup_s": setup_s,
     }
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(X, solvers["fp64"], w, row, col, val, b,
-                                           res["fp64"]["iters"], args)
+        cb, errs, oit = cpu_baseline(solvers["fp64"], w, row, col, val, b,
+                                     {k: v["x"] for k, v in res.items()})
+        out["cpu_baseline"] = cb
+        out["rel_err_vs_oracle"] = errs
+        out["iters"]["oracle_fp64"] = oit
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -323,91 +330,170 @@ def roofline(X, torch, stream, S, n, nv, args, which=3, reps=50):
             "launches_timed": reps}
 
 
-class OracleArm:
-    """The oracle on the host (the restatement of XAMG's FP64 CPU solve): the
-    same plain-FP64 solve on the same hierarchy, cut to a bounded sample of
-    `sample_iters` outer iterations per step."""
+def config_of(w, n, nnz):
+    """The workload description both arms print (same keys, same values)."""
+    return {"workload": w["desc"], "rows": n, "nnz": int(nnz), "nv": w["nv"],
+            "rhs_per_gpu_per_step": w["nv"], "tolerance": 1e-8,
+            "l2": "inputs larger than L2 (matrix > 126 MB)" if nnz * 12 > 126e6
+            else "L2-resident inputs (no flush)"}
 
-    def __init__(self, S, w, row, col, val, b, sample_iters):
-        sys.path.insert(0, os.path.join(ROOT, "tests"))
-        import oracle_py as O
+
+def oracle_module():
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_py
+    return oracle_py
+
+
+class OracleSolve:
+    """The oracle (the restatement of XAMG's FP64 CPU solve phase) set up for
+    the plain-FP64 method of workload w on a given hierarchy: full solves from
+    x = 0 to the relative tolerance, dot products in XAMG's order over one
+    core range per host thread (as XAMG's ranks sum them), every loop on the
+    host threads."""
+
+    def __init__(self, w, row, col, val, hierarchy):
+        O = oracle_module()
+        self.O = O
         self.nv = w["nv"]
-        p = json.loads(json.dumps(params_for(w, False)))
-        p["solver"]["max_iters"] = sample_iters
-        p["solver"]["rel_tolerance"] = 0.0
         self.sysm = O.System(self.nv)
-        self.sysm.set_params(p)
-        if w["smoother"] is None:
+        self.sysm.set_params(params_for(w, False))
+        if hierarchy is None:
             self.sysm.add_level(row, col, val)
         else:
-            # the hierarchy the GPU solver uses (the oracle applies XAMG's
-            # parse and setup on it)
-            for lv in S.hierarchy():
+            for lv in hierarchy:
                 self.sysm.add_level(*lv["A"], lv["min_eig"], lv["max_eig"])
                 if lv["P"] is not None:
                     self.sysm.add_interp(*lv["P"])
         self.sysm.setup()
-        self.b = b
         self.cores = O.threads()
 
-    def step(self):
-        """Seconds per outer iteration of one sampled solve."""
-        t0 = time.perf_counter()
-        _, st = self.sysm.solve(self.b)
-        dt = time.perf_counter() - t0
-        self.last = (dt, st["iters"])
-        return dt / max(1, st["iters"])
+    def solve(self, b):
+        """(x, stats, seconds) of one whole solve."""
+        self.O.set_reduction(0, self.cores)
+        try:
+            t0 = time.perf_counter()
+            x, st = self.sysm.solve(b)
+            return x, st, time.perf_counter() - t0
+        finally:
+            self.O.set_reduction(0)
 
 
-def cpu_baseline(X, S, w, row, col, val, b, iters_full, args):
-    """A bounded sample of the plain-FP64 solve on the oracle, scaled to the
-    full iteration count."""
-    arm = OracleArm(S, w, row, col, val, b, args.cpu_iters)
-    per_iter = arm.step()
-    dt, it = arm.last
-    ms_rhs = per_iter * iters_full * 1e3 / w["nv"]
-    return {"value": ms_rhs, "unit": "ms/RHS", "cores": arm.cores, "kind": "port",
-            "sample": f"{it} outer iterations of the plain-FP64 solve "
-                      f"({dt:.1f} s), scaled to the GPU's {iters_full} iterations"}
+def oracle_inputs(w):
+    """Matrix, right-hand side and hierarchy of workload w without the CUDA
+    library: the seeded generators and the host multigrid setup compiled into
+    oracle/liboracle_setup.so from the library's host-only sources."""
+    O = oracle_module()
+    g = w["grid"]
+    if w["stencil"] == 0:
+        row, col, val = O.generate_cube(g, g, g)
+    else:
+        row, col, val = O.setup_generate_diffusion(w["stencil"], g, g, g, w["sigma"], w["aniso"], 0)
+    n = len(row) - 1
+    b = np.random.default_rng(1000).uniform(-1, 1, n * w["nv"])
+    H = None
+    if w["smoother"] is not None:
+        H = O.setup_hierarchy(row, col, val, params_for(w, False)["preconditioner"])
+    return row, col, val, b, H
+
+
+def rel_err(x, ref, nv):
+    """max over right-hand sides of ||x - ref|| / ||ref||"""
+    X, R = x.reshape(-1, nv), ref.reshape(-1, nv)
+    return float((np.linalg.norm(X - R, axis=0) / np.linalg.norm(R, axis=0)).max())
+
+
+def cpu_baseline(S, w, row, col, val, b, xs):
+    """One whole plain-FP64 solve of the same system on the oracle (the
+    hierarchy the GPU solver built), timed on the host threads; its solution
+    gives each GPU result's relative error against the FP64 CPU oracle."""
+    arm = OracleSolve(w, row, col, val, S.hierarchy() if w["smoother"] else None)
+    x, st, dt = arm.solve(b)
+    cb = {"value": dt * 1e3 / w["nv"], "unit": "ms/RHS", "cores": arm.cores, "kind": "port",
+          "sample": f"one whole plain-FP64 solve of the same {w['nv']} right-hand sides to 1e-8 "
+                    f"({st['iters']} iterations, {dt:.1f} s), XAMG's reduction order over "
+                    f"{arm.cores} core ranges"}
+    errs = {k: rel_err(v, x, w["nv"]) for k, v in xs.items()}
+    return cb, errs, int(st["iters"])
+
+
+class quiet_stdout:
+    """Sends what native code prints to stdout (the reference's log lines)
+    to stderr, so that stdout carries only the JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *a):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
 
 
 def run_reference(args, w):
-    """CPU arm: the oracle's plain-FP64 solve (C++, SpMV rows on all host
-    threads), each step one sampled outer iteration of the full-size solve
-    scaled to the iteration count the solve needs; one untimed warm-up step,
-    median of K."""
+    """CPU arm, alone in this process (no CUDA library, no GPU): the
+    reference's own solve phase, XAMG's C API compiled unmodified from its
+    sources into oracle/_ref with single-process stand-ins for MPI,
+    argsparser's parameter dictionary and hypre (one rank: one core), on the
+    same matrix, right-hand sides and hierarchy (oracle/liboracle_setup.so;
+    the hierarchy is registered with the hypre stand-in). Each step is one
+    whole plain-FP64 solve of the nv right-hand sides from x = 0 to the
+    tolerance; whole solves take tens of seconds at full size, so after
+    min(W, 1) warm-up solves it times at most K solves within a time budget
+    and reports the number it timed. Without oracle/_ref (no reference
+    sources where it was built) the oracle port on all host threads stands
+    in (kind "port"). Under torchrun only rank 0 runs it."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return None
-    import xamg_b200 as X
-    X.init()
-    row, col, val = make_matrix(X, w)
-    n = len(row) - 1
-    b = np.random.default_rng(1000).uniform(-1, 1, n * w["nv"])
-    M = X.Matrix(row, col, val)
-    xv, bv = X.Vector(n, w["nv"]), X.Vector(n, w["nv"])
-    bv.upload(b)
-    xv.set(0.0)
-    S = X.Solver(M, X.Params(params_for(w, False)), xv, bv)
-    S.solve()
-    iters = S.stats()["iters"]
-    arm = OracleArm(S, w, row, col, val, b, args.cpu_iters)
-    for _ in range(min(args.warmup, 1)):
-        arm.step()
-    vals = [arm.step() * iters * 1e3 / w["nv"] for _ in range(args.steps)]
-    v = float(np.median(vals))
-    dt, it = arm.last
-    cb = {"value": v, "unit": "ms/RHS", "cores": arm.cores, "kind": "port",
-          "sample": f"per step {it} outer iteration(s) of the plain-FP64 solve ({dt:.1f} s), "
-                    f"scaled to the {iters} iterations of the full solve; median of "
-                    f"{args.steps} steps"}
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import ref_capi
+    t0 = time.time()
+    row, col, val, b, H = oracle_inputs(w)
+    n, nv = len(row) - 1, w["nv"]
+    use_ref = ref_capi.available(nv)
+    with quiet_stdout():
+        if use_ref:
+            S = ref_capi.Solve(row, col, val, nv, params_for(w, False), hierarchy=H)
+            def one():
+                x, conv = S.solve(b)
+                return x, int(conv.sum()), S.last_seconds
+            cores, kind = 1, "reference"
+        else:
+            arm = OracleSolve(w, row, col, val, H)
+            def one():
+                x, st, dt = arm.solve(b)
+                return x, int(st["conv"].sum()), dt
+            cores, kind = arm.cores, "port"
+        setup_s = time.time() - t0
+        warm = min(args.warmup, 1)
+        for _ in range(warm):
+            one()
+        total, steps, budget = 0.0, 0, 90.0
+        while steps < args.steps and (steps == 0 or total < budget):
+            x, nconv, dt = one()
+            total += dt
+            steps += 1
+    v = total * 1e3 / (steps * nv)
+    import scipy.sparse as sp
+    A = sp.csr_matrix((val, col, row), shape=(n, n))
+    Xs, Bs = x.reshape(n, nv), b.reshape(n, nv)
+    true_rel = (np.linalg.norm(Bs - A @ Xs, axis=0) / np.linalg.norm(Bs, axis=0)).max()
+    what = ("XAMG's own solve phase built from the reference sources, one rank"
+            if use_ref else "the oracle port, XAMG's reduction order over the host threads")
+    cb = {"value": v, "unit": "ms/RHS", "cores": cores, "kind": kind,
+          "sample": f"each step one whole plain-FP64 solve of the {nv} right-hand sides to 1e-8 "
+                    f"({what}); {steps} steps timed after {warm} warm-up, "
+                    f"{nconv}/{nv} right-hand sides converged"}
     return {"impl": "reference",
             "metric": "ms/RHS to 1e-8 residual: chosen vs plain FP64 on 1 B200; SpMV % of HBM BW",
-            "value": v, "unit": "ms/RHS", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": v * w["nv"], "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": w["desc"], "rows": n, "nv": w["nv"]},
-            "cpu_baseline": cb,
+            "value": v, "unit": "ms/RHS", "n_gpus": ws, "steps": steps, "steps_requested": args.steps,
+            "warmup": warm, "ms_per_step": total * 1e3 / steps,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": config_of(w, n, len(col)),
+            "true_rel_residual": float(true_rel), "setup_s": setup_s, "cpu_baseline": cb,
             "e2e": {"value": v, "unit": "ms/RHS", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
 
@@ -590,7 +676,6 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="amg27", choices=sorted(WORKLOADS))
     ap.add_argument("--grid", type=int, default=None, help="override the grid edge")
-    ap.add_argument("--cpu-iters", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--roofline-only", action="store_true",
                     help="set up, then time only the level-0 SpMV (--steps launches): "

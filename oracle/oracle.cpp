@@ -800,6 +800,29 @@ static Csr to_f32(const Csr &a) {
     return b;
 }
 
+// B200 extension gpu_level_bf16: a float level operator whose values are
+// stored in BF16. Each float value is rounded to the nearest BF16 (ties to
+// even: add 0x7FFF plus the lowest kept bit, then drop the low 16 bits; NaN
+// stays NaN) and used as that float.
+static float round_bf16(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    if ((u & 0x7F800000u) == 0x7F800000u && (u & 0x007FFFFFu)) {
+        u |= 0x00400000u;  // quiet NaN
+    } else {
+        u += 0x7FFFu + ((u >> 16) & 1u);
+    }
+    u &= 0xFFFF0000u;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+
+static Csr to_bf16_values(const Csr &a) {
+    Csr b = a;
+    for (float &v : b.vf) v = round_bf16(v);
+    return b;
+}
+
 // csr_matrix.inl:86-170
 static void compress(Csr &m) {
     if (m.empty()) return;
@@ -1233,6 +1256,8 @@ static SolverParams resolve(const Params &P, const std::string &role, int level)
 
 struct Level {
     Csr A;                    // in the level's working precision
+    Csr Abf;                  // A with BF16-rounded values (gpu_level_bf16), else empty
+    bool bf16 = false;        // the cycle's and smoothers' SpMVs use Abf
     Csr R, P;                 // transfer to level+1 (absent on the coarsest level)
     double min_eig = NAN, max_eig = NAN;
     bool reduced = false;     // working precision is float
@@ -1266,6 +1291,7 @@ struct Solver {
     std::shared_ptr<Solver> coarse;
     std::shared_ptr<Solver> precond;
     std::vector<std::vector<Vec>> mgbuf;  // per level buffers (mg.inl:136-163)
+    Vec mg_b32, mg_x32;                   // float input/output (gpu_precond_f32 = 1)
 };
 
 template <typename T>
@@ -1588,7 +1614,7 @@ static void mg_cycle(Solver &S, Vec &x, Vec &b, int level, int cycle, const Vec 
     const int NV = S.NV;
     Vec a1 = typed_scalar<T1>(NV, 1.0), a_1 = typed_scalar<T1>(NV, -1.0);
     Vec iconv2 = make_vec<T2>(1, NV);
-    Csr &A = L[level].A;
+    Csr &A = L[level].bf16 ? L[level].Abf : L[level].A;
     Csr &R = L[level].R;
     Csr &P = L[level].P;
     Vec &temp = S.mgbuf[level][0];
@@ -1645,8 +1671,14 @@ static void solve_mg(Solver &S, Vec &x, Vec &b, const Vec &conv) {
     if ((*S.levels)[0].reduced) {
         // B200 extension (gpu_precond_f32 = 1, preconditioner only): every
         // level in float, the input converted on entry and the result on exit
+        // the float copies persist between applications, as the B200
+        // library's do (an F-cycle's prolongation reads x32's old contents)
         const uint64_t n = (*S.levels)[0].A.nrows;
-        Vec b32 = make_vec<float>(n, NV), x32 = make_vec<float>(n, NV);
+        if (S.mg_b32.size != n) {
+            S.mg_b32 = make_vec<float>(n, NV);
+            S.mg_x32 = make_vec<float>(n, NV);
+        }
+        Vec &b32 = S.mg_b32, &x32 = S.mg_x32;
         Vec ic32 = make_vec<float>(1, NV);
         convert_vec<double>(b, b32);
         convert_vec<double>(x, x32);
@@ -1996,13 +2028,15 @@ static int buffer_nvecs(const std::string &m) {
     return 0;
 }
 
+// op: the matrix the solver's SpMVs use when it differs from A (a BF16-valued
+// level operator); diagonals and the other setup read A.
 static std::shared_ptr<Solver> make_basic(System &sys, const std::string &role, int level,
                                           const Csr &A, bool f32, double min_eig,
-                                          double max_eig) {
+                                          double max_eig, const Csr *op = nullptr) {
     auto S = std::make_shared<Solver>();
     S->sp = resolve(sys.P, role, level);
     S->method = S->sp.method;
-    S->A = &A;
+    S->A = op ? op : &A;
     S->f32 = f32;
     S->NV = sys.NV;
     S->min_eig = min_eig;
@@ -2056,7 +2090,10 @@ static int setup(System &sys) {
     const bool mg_prec = (pre == "MultiGrid");
     const std::string mg_role = mg_solver ? "solver" : "preconditioner";
     bool reduced = false, full32 = false;
+    int bf16_levels = 0;
     if (mg_solver || mg_prec) {
+        std::string bf = sys.P.get(mg_role, "gpu_level_bf16");
+        if (!bf.empty()) bf16_levels = (int)std::stol(bf);
         std::string v = sys.P.get(mg_role, "mg_reduced_precision");
         reduced = !v.empty() && std::stol(v) != 0;
         // B200 extension: gpu_precond_f32 = 1 puts the finest level of the
@@ -2075,6 +2112,10 @@ static int setup(System &sys) {
         Level &lv = sys.levels[l];
         lv.reduced = (l >= 1 || full32) && reduced;
         lv.A = lv.reduced ? to_f32(sys.A64[l]) : sys.A64[l];
+        // gpu_level_bf16: the finest float cycle operators store BF16 values
+        // (the smoothers' diagonals and the transfers keep the float values)
+        lv.bf16 = lv.reduced && (int)l < bf16_levels;
+        if (lv.bf16) lv.Abf = to_bf16_values(lv.A);
         lv.min_eig = sys.min_eig[l];
         lv.max_eig = sys.max_eig[l];
         if (l + 1 < L) {
@@ -2093,14 +2134,15 @@ static int setup(System &sys) {
         M->levels = &sys.levels;
         for (size_t nl = 0; nl + 1 < L; ++nl) {
             Level &lv = sys.levels[nl];
+            const Csr *op = lv.bf16 ? &lv.Abf : nullptr;
             M->pre.push_back(make_basic(sys, "pre_smoother", (int)nl, lv.A, lv.reduced,
-                                        lv.min_eig, lv.max_eig));
+                                        lv.min_eig, lv.max_eig, op));
             M->post.push_back(make_basic(sys, "post_smoother", (int)nl, lv.A, lv.reduced,
-                                         lv.min_eig, lv.max_eig));
+                                         lv.min_eig, lv.max_eig, op));
         }
         Level &cl = sys.levels[L - 1];
         M->coarse = make_basic(sys, "coarse_grid_solver", -1, cl.A, cl.reduced, cl.min_eig,
-                               cl.max_eig);
+                               cl.max_eig, cl.bf16 ? &cl.Abf : nullptr);
         M->mgbuf.resize(L);
         for (size_t nl = 0; nl < L; ++nl) {
             const uint64_t n = sys.levels[nl].A.nrows;
@@ -2309,6 +2351,11 @@ void or_inv_diag(int f32, int sqrt_, uint64_t nrows, uint64_t nnz, const uint32_
 void or_cheby_coeffs(double min_eig, double max_eig, int order, float frac, double *out) {
     auto c = cheby_coeffs(min_eig, max_eig, order, (double)frac);
     for (int i = 0; i < order; ++i) out[i] = c[i];
+}
+
+// BF16 rounding of float values (gpu_level_bf16 operators)
+void or_round_bf16(uint64_t n, const float *in, float *out) {
+    for (uint64_t i = 0; i < n; ++i) out[i] = round_bf16(in[i]);
 }
 
 // dot products in the configured reduction order (double)

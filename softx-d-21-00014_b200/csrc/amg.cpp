@@ -21,9 +21,11 @@
 //    (Lanczos tridiagonal eigenvalues), as hypre does for relax type 16.
 //
 // Parameters read: mg_strength_threshold, mg_max_row_sum, mg_trunc_factor,
-// mg_Pmax_elements, mg_max_levels, mg_coarse_matrix_size, gpu_seed. All
-// coarsening types use PMIS and all interpolation types use extended+i;
-// aggressive coarsening levels are not built.
+// mg_Pmax_elements, mg_max_levels, mg_coarse_matrix_size, gpu_seed. Only
+// PMIS coarsening (hypre type 8) and extended+i interpolation (type 6) without
+// aggressive levels are implemented; the multigrid setup in solver.cu refuses
+// any other mg_coarsening_type, mg_interpolation_type or mg_agg_num_levels
+// with XAMG_ERR_UNSUPPORTED before calling build_hierarchy.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>

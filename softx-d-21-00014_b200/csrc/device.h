@@ -113,14 +113,11 @@ struct DVec {
     bool init = false;
     std::shared_ptr<DevBuf> buf;
 
-    void alloc(uint64_t n_, int nv_, bool f32_) {
-        n = n_;
-        nv = nv_;
-        f32 = f32_;
-        buf = std::make_shared<DevBuf>(n * nv * (f32 ? 4 : 8));
-        zero = true;
-        init = false;
-    }
+    // New vectors start with zero contents (as XAMG's zero-flagged vectors
+    // do in host memory): kernels that accumulate into a vector's memory
+    // whatever its flag says (the F-cycle's prolongation) then read the
+    // same values the reference reads.
+    void alloc(uint64_t n_, int nv_, bool f32_);
     template <typename T>
     T *p() const {
         return buf ? (T *)buf->p : nullptr;

@@ -17,6 +17,19 @@ Ctx &ctx() {
 
 Ctx &ctx_uninit() { return g_ctx; }
 
+void DVec::alloc(uint64_t n_, int nv_, bool f32_) {
+    n = n_;
+    nv = nv_;
+    f32 = f32_;
+    buf = std::make_shared<DevBuf>(n * nv * (f32 ? 4 : 8));
+    if (buf->bytes) {
+        XG_CUDA(cudaMemsetAsync(buf->p, 0, buf->bytes, ctx().stream));
+        XG_CUDA(cudaStreamSynchronize(ctx().stream));
+    }
+    zero = true;
+    init = false;
+}
+
 // Creates a lane's stream, scratch and pinned slots (the fields of Ctx or of
 // a parked Lane).
 static void lane_create(cudaStream_t &stream, DevBuf &part, DevBuf &ticket, DevBuf &out,

@@ -1,6 +1,7 @@
 // Parameter dictionary (see params.h).
 #include "params.h"
 
+#include <cmath>
 #include <cstdlib>
 #include <sstream>
 
@@ -37,46 +38,47 @@ float PList::get_f(const std::string &k, float def) const {
     return std::strtof(it->second.s.c_str(), nullptr);
 }
 
-// xamg_params_details.h:79-123, plus the B200 keys
+// xamg_params_details.h:79-123 (type, families, min/max, allowed values),
+// plus the B200 keys
 static const std::map<std::string, KeyInfo> &dictionary() {
     static const std::map<std::string, KeyInfo> d = {
-        {"method", {'S', ""}},
-        {"convergence_check", {'I', "!Identity,!Direct"}},
-        {"convergence_info", {'I', "!Identity,!Direct"}},
-        {"polynomial_order", {'I', "Chebyshev"}},
-        {"spectrum_fraction", {'F', "Chebyshev"}},
-        {"max_iters", {'I', "!Identity,!Direct"}},
-        {"abs_tolerance", {'F', "!Identity,!Direct"}},
-        {"rel_tolerance", {'F', "!Identity,!Direct"}},
-        {"relax_factor", {'F', "Jacobi,HSGS"}},
-        {"hypre_log", {'I', "MultiGrid"}},
-        {"hypre_per_level_hierarchy", {'I', "MultiGrid"}},
-        {"mg_reduced_precision", {'I', "MultiGrid"}},
-        {"mg_cycle", {'I', "MultiGrid"}},
-        {"mg_max_levels", {'I', "MultiGrid"}},
-        {"mg_coarse_matrix_size", {'I', "MultiGrid"}},
-        {"mg_strength_threshold", {'F', "MultiGrid"}},
-        {"mg_trunc_factor", {'F', "MultiGrid"}},
-        {"mg_num_paths", {'I', "MultiGrid"}},
-        {"mg_coarsening_type", {'I', "MultiGrid"}},
-        {"mg_interpolation_type", {'I', "MultiGrid"}},
-        {"mg_Pmax_elements", {'I', "MultiGrid"}},
-        {"mg_max_row_sum", {'F', "MultiGrid"}},
-        {"mg_nonGalerkin_tol", {'F', "MultiGrid"}},
-        {"mg_agg_num_levels", {'I', "MultiGrid"}},
-        {"mg_agg_interpolation_type", {'I', "MultiGrid"}},
-        {"mg_agg_trunc_factor", {'F', "MultiGrid"}},
-        {"mg_agg_P12_trunc_factor", {'F', "MultiGrid"}},
-        {"mg_agg_Pmax_elements", {'I', "MultiGrid"}},
-        {"mg_agg_P12max_elements", {'I', "MultiGrid"}},
-        {"gpu_precond_f32", {'I', ""}},
-        {"gpu_coarse_f64", {'I', ""}},
-        {"gpu_index_compress", {'I', ""}},
-        {"gpu_hsgs_rows", {'I', ""}},
-        {"gpu_graph", {'I', ""}},
-        {"gpu_spmv_tune", {'I', ""}},
-        {"gpu_level_bf16", {'I', ""}},
-        {"gpu_seed", {'I', ""}},
+        {"method", {'S', "", "", "", ""}},
+        {"convergence_check", {'I', "!Identity,!Direct", "0", "1", ""}},
+        {"convergence_info", {'I', "!Identity,!Direct", "0", "1", ""}},
+        {"polynomial_order", {'I', "Chebyshev", "1", "4", ""}},
+        {"spectrum_fraction", {'F', "Chebyshev", "0.0", "1.0", ""}},
+        {"max_iters", {'I', "!Identity,!Direct", "0", "inf", ""}},
+        {"abs_tolerance", {'F', "!Identity,!Direct", "0.0", "inf", ""}},
+        {"rel_tolerance", {'F', "!Identity,!Direct", "0.0", "inf", ""}},
+        {"relax_factor", {'F', "Jacobi,HSGS", "", "", ""}},
+        {"hypre_log", {'I', "MultiGrid", "0", "1", ""}},
+        {"hypre_per_level_hierarchy", {'I', "MultiGrid", "0", "1", ""}},
+        {"mg_reduced_precision", {'I', "MultiGrid", "0", "1", ""}},
+        {"mg_cycle", {'I', "MultiGrid", "", "", "0,1,2"}},
+        {"mg_max_levels", {'I', "MultiGrid", "1", "50", ""}},
+        {"mg_coarse_matrix_size", {'I', "MultiGrid", "1", "2000", ""}},
+        {"mg_strength_threshold", {'F', "MultiGrid", "0.0", "1.0", ""}},
+        {"mg_trunc_factor", {'F', "MultiGrid", "0.0", "1.0", ""}},
+        {"mg_num_paths", {'I', "MultiGrid", "1", "10", ""}},
+        {"mg_coarsening_type", {'I', "MultiGrid", "0", "22", "0,1,3,6,7,8,9,10,11,21,22"}},
+        {"mg_interpolation_type", {'I', "MultiGrid", "0", "14", ""}},
+        {"mg_Pmax_elements", {'I', "MultiGrid", "0", "inf", ""}},
+        {"mg_max_row_sum", {'F', "MultiGrid", "0.0", "1.0", ""}},
+        {"mg_nonGalerkin_tol", {'F', "MultiGrid", "0.0", "1.0", ""}},
+        {"mg_agg_num_levels", {'I', "MultiGrid", "0", "50", ""}},
+        {"mg_agg_interpolation_type", {'I', "MultiGrid", "1", "4", ""}},
+        {"mg_agg_trunc_factor", {'F', "MultiGrid", "0.0", "1.0", ""}},
+        {"mg_agg_P12_trunc_factor", {'F', "MultiGrid", "0.0", "1.0", ""}},
+        {"mg_agg_Pmax_elements", {'I', "MultiGrid", "0", "inf", ""}},
+        {"mg_agg_P12max_elements", {'I', "MultiGrid", "0", "inf", ""}},
+        {"gpu_precond_f32", {'I', "", "0", "1", ""}},
+        {"gpu_coarse_f64", {'I', "", "0", "1", ""}},
+        {"gpu_index_compress", {'I', "", "0", "2", ""}},
+        {"gpu_hsgs_rows", {'I', "", "1", "inf", ""}},
+        {"gpu_graph", {'I', "", "0", "1", ""}},
+        {"gpu_spmv_tune", {'I', "", "0", "1", ""}},
+        {"gpu_level_bf16", {'I', "", "0", "50", ""}},
+        {"gpu_seed", {'I', "", "", "", ""}},
     };
     return d;
 }
@@ -104,8 +106,38 @@ static void check_key(const std::string &key) {
     XG_REQUIRE(key_info(key) != nullptr, XAMG_ERR_INVALID_ARG, "unknown parameter key: " + key);
 }
 
+// The value's range and allowed set (xamg_params_details.h:79-123): integer
+// keys compare as the stored uint16, float keys as the stored float32.
+static void check_value(const std::string &key, const PValue &v) {
+    const KeyInfo *ki = key_info(key);
+    if (!ki || ki->type == 'S') return;
+    const double x = v.type == 'I'   ? (double)v.i
+                     : v.type == 'F' ? (double)v.f
+                                     : std::strtod(v.s.c_str(), nullptr);
+    XG_REQUIRE(!std::isnan(x), XAMG_ERR_INVALID_ARG,
+               "parameter " + key + " is NaN");
+    const std::string mn = ki->min, mx = ki->max;
+    if (!mn.empty())
+        XG_REQUIRE(x >= (double)std::strtof(mn.c_str(), nullptr), XAMG_ERR_INVALID_ARG,
+                   "parameter " + key + " = " + v.str() + " is below its minimum " + mn);
+    if (!mx.empty() && mx != "inf")
+        XG_REQUIRE(x <= (double)std::strtof(mx.c_str(), nullptr), XAMG_ERR_INVALID_ARG,
+                   "parameter " + key + " = " + v.str() + " is above its maximum " + mx);
+    const std::string al = ki->allowed;
+    if (!al.empty()) {
+        bool ok = false;
+        std::stringstream ss(al);
+        std::string a;
+        while (std::getline(ss, a, ','))
+            if (x == (double)std::strtof(a.c_str(), nullptr)) ok = true;
+        XG_REQUIRE(ok, XAMG_ERR_INVALID_ARG,
+                   "parameter " + key + " = " + v.str() + " is not one of {" + al + "}");
+    }
+}
+
 void Params::add_value(const std::string &role, const std::string &key, const PValue &v) {
     check_key(key);
+    check_value(key, v);
     lists[role].set(key, v);
 }
 
@@ -114,12 +146,14 @@ void Params::change_value(const std::string &role, const std::string &key, const
     auto it = lists.find(role);
     XG_REQUIRE(it != lists.end() && it->second.has(key), XAMG_ERR_INVALID_ARG,
                "change_value: " + role + "." + key + " is not set");
+    check_value(key, v);
     it->second.set(key, v);
 }
 
 void Params::forced_change_value(const std::string &role, const std::string &key,
                                  const PValue &v) {
     check_key(key);
+    check_value(key, v);
     lists[role].set(key, v);
 }
 
@@ -145,6 +179,7 @@ void Params::add_override(const std::string &role, const std::map<std::string, s
             }
             XG_REQUIRE(a >= 0 && b >= a && b < 50, XAMG_ERR_INVALID_ARG,
                        "override level range out of 0..49: " + spec);
+            check_value(kvp.first, parse_typed(kvp.first, val));
             for (int l = a; l <= b; ++l) overrides[role][l][kvp.first] = val;
         }
     }

@@ -30,11 +30,14 @@ struct PList {
     void set(const std::string &k, const PValue &v) { kv[k] = v; }
 };
 
-// Keys the dictionary knows, with value type and the families they apply to
-// (xamg_params_details.h:79-123).
+// Keys the dictionary knows, with value type, the families they apply to,
+// and the value range and allowed set (xamg_params_details.h:79-123).
 struct KeyInfo {
     char type;
     const char *families;  // comma-separated; "!X" excludes; empty = all
+    const char *min;       // "" = no bound
+    const char *max;       // "" or "inf" = no bound
+    const char *allowed;   // comma-separated allowed values; "" = any in range
 };
 const KeyInfo *key_info(const std::string &key);
 

@@ -487,6 +487,24 @@ void MultiGrid::build(const HCsr &A0, const DCsr *A0dev, const Params &P, const 
     if (cache && cache->count(key)) {
         H = (*cache)[key];
     } else {
+        // The host setup implements PMIS coarsening (hypre type 8) with
+        // extended+i interpolation (type 6) and no aggressive levels; hypre
+        // offers more (hypre_base.h:155-163). Other choices, on any level the
+        // hierarchy can reach, are refused rather than replaced.
+        for (int l = 0; l < std::max(1, cfg.mg_max_levels); ++l) {
+            const SolverCfg c = resolve_cfg(P.get(role, l), role);
+            XG_REQUIRE(c.mg_coarsening_type == 8, XAMG_ERR_UNSUPPORTED,
+                       "mg_coarsening_type " + std::to_string(c.mg_coarsening_type) +
+                           " (level " + std::to_string(l) +
+                           "): only PMIS (8) is implemented by the host setup");
+            XG_REQUIRE(c.mg_interpolation_type == 6, XAMG_ERR_UNSUPPORTED,
+                       "mg_interpolation_type " + std::to_string(c.mg_interpolation_type) +
+                           " (level " + std::to_string(l) +
+                           "): only extended+i (6) is implemented by the host setup");
+            XG_REQUIRE(c.mg_agg_num_levels == 0, XAMG_ERR_UNSUPPORTED,
+                       "mg_agg_num_levels " + std::to_string(c.mg_agg_num_levels) +
+                           ": aggressive coarsening is not implemented by the host setup");
+        }
         H = std::make_shared<const Hierarchy>(build_hierarchy(A0, cfg));
         if (cache) (*cache)[key] = H;
     }
@@ -617,14 +635,11 @@ void MultiGrid::cycle(int level, DVec &x, DVec &b, int cyc, const std::vector<do
         if (mixed) {
             ops::prolong_mixed(lv.P, xH.p<float>(), x.p<double>(), x.zero, NV, S());
         } else {
-            // Axpy(P, x_H, x) accumulates into x; a zero-flagged x is written
-            // with zeros first so that no stale contents are read
-            if (x.zero) {
-                if (lv.f32)
-                    ops::fill<float>(x.p<float>(), x.elems(), 0.f, S());
-                else
-                    ops::fill<double>(x.p<double>(), x.elems(), 0.0, S());
-            }
+            // Axpy(P, x_H, x) accumulates into x's memory whatever its zero
+            // flag says (blas2.h:284-326, csr_matvec.inl:33-144): after the
+            // F-cycle's first visit of a level (no pre-smoothing,
+            // mg.inl:198) x still holds what the previous cycle left in it,
+            // and the reference adds to that
             if (lv.f32)
                 ops::spmv<float>(lv.P, xH.p<float>(), x.p<float>(), NV, true, S());
             else

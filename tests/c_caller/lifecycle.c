@@ -115,6 +115,12 @@ int main(int argc, char **argv) {
     CHECK(XAMG_param_add_value_d("solver", "abs_tolerance", 0.0f, par));
     CHECK(XAMG_param_add_value_s("preconditioner", "method", "MultiGrid", par));
     CHECK(XAMG_param_add_value_i("preconditioner", "mg_coarse_matrix_size", 50, par));
+    /* the host setup implements PMIS (8) with extended+i (6), no aggressive levels */
+    CHECK(XAMG_param_add_value_i("preconditioner", "mg_coarsening_type", 8, par));
+    CHECK(XAMG_param_add_value_i("preconditioner", "mg_interpolation_type", 6, par));
+    CHECK(XAMG_param_add_value_i("preconditioner", "mg_agg_num_levels", 0, par));
+    /* out-of-range values are refused (polynomial_order is 1..4) */
+    if (XAMG_param_add_value_i("pre_smoother", "polynomial_order", 9, par) == 0) return 3;
     XAMG_param_override_id ov;
     CHECK(XAMG_param_override_create(&ov));
     CHECK(XAMG_param_override_add_value("mg_coarsening_type", "8@lev0-1", ov));

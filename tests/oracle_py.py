@@ -59,6 +59,7 @@ def lib():
         L.or_group1.argtypes = [C.c_uint64, C.c_int, f64p, f64p, f64p, f64p, f64p]
         L.or_group2.argtypes = [C.c_uint64, C.c_int, f64p, f64p, f64p, f64p, f64p]
         L.or_group4.argtypes = [C.c_uint64, C.c_int, f64p, f64p, f64p, f64p, f64p, f64p]
+        L.or_round_bf16.argtypes = [C.c_uint64, C.c_void_p, C.c_void_p]
         L.or_threads.restype = C.c_int
         L.or_generate_cube.restype = C.c_uint64
         L.or_generate_cube.argtypes = [C.c_uint64] * 3 + [u32p, u32p, f64p]
@@ -167,6 +168,14 @@ def inv_diag(row, col, val, f32=False, sqrt=False):
 def cheby_coeffs(min_eig, max_eig, order, frac):
     out = np.zeros(order, np.float64)
     lib().or_cheby_coeffs(min_eig, max_eig, order, frac, out)
+    return out
+
+
+def round_bf16(a):
+    """float32 array -> the same values rounded to BF16 (as float32)"""
+    a = np.ascontiguousarray(a, np.float32)
+    out = np.empty_like(a)
+    lib().or_round_bf16(a.size, a.ctypes.data, out.ctypes.data)
     return out
 
 

@@ -136,3 +136,45 @@ def test_no_cpu_fallback(xamg):
     v = C.c_size_t()
     assert xamg.lib().XAMG_vector_create(C.byref(v), 2) == 0
     assert xamg.lib().XAMG_vector_alloc_d(10, 1, v.value) == -4
+
+
+def test_param_ranges_and_allowed_sets(xamg):
+    """Values outside the ranges and allowed sets of
+    xamg_params_details.h:79-123 are refused with XAMG_ERR_INVALID_ARG by
+    add, change, forced change and per-level overrides; boundary values are
+    accepted."""
+    L = xamg.lib()
+    p = xamg.Params({"solver": {"method": "PBiCGStab"},
+                     "preconditioner": {"method": "MultiGrid"},
+                     "pre_smoother": {"method": "Chebyshev"}}, set_default=False)
+    bad = [("pre_smoother", "polynomial_order", 0), ("pre_smoother", "polynomial_order", 5),
+           ("pre_smoother", "spectrum_fraction", 1.5), ("preconditioner", "mg_cycle", 3),
+           ("preconditioner", "mg_coarsening_type", 2), ("preconditioner", "mg_coarsening_type", 23),
+           ("preconditioner", "mg_max_levels", 0), ("preconditioner", "mg_max_levels", 51),
+           ("preconditioner", "mg_coarse_matrix_size", 2001),
+           ("preconditioner", "mg_strength_threshold", -0.1),
+           ("preconditioner", "mg_agg_interpolation_type", 0), ("solver", "rel_tolerance", -1e-8),
+           ("solver", "convergence_check", 2), ("preconditioner", "gpu_index_compress", 3)]
+    for role, key, value in bad:
+        with pytest.raises(xamg.XamgError) as e:
+            p.add(role, key, value)
+        assert e.value.code == -2, (key, value)
+        with pytest.raises(xamg.XamgError):
+            p.change(role, key, value, forced=True)
+    good = [("pre_smoother", "polynomial_order", 1), ("pre_smoother", "polynomial_order", 4),
+            ("pre_smoother", "spectrum_fraction", 1.0), ("preconditioner", "mg_cycle", 2),
+            ("preconditioner", "mg_coarsening_type", 22), ("preconditioner", "mg_max_levels", 50),
+            ("preconditioner", "mg_coarse_matrix_size", 2000), ("solver", "max_iters", 65535),
+            ("preconditioner", "gpu_index_compress", 2)]
+    for role, key, value in good:
+        p.add(role, key, value)
+    p.change("preconditioner", "mg_cycle", 1)
+    with pytest.raises(xamg.XamgError):
+        p.change("preconditioner", "mg_cycle", 4)
+    for spec in ("3@lev0", "1@lev2-4"):
+        o = C.c_size_t()
+        assert L.XAMG_param_override_create(C.byref(o)) == 0
+        assert L.XAMG_param_override_add_value(b"mg_cycle", spec.encode(), o.value) == 0
+        rc = L.XAMG_param_override_apply(b"preconditioner", p.h, o.value)
+        assert rc == (-2 if spec.startswith("3") else 0), spec
+        L.XAMG_param_override_destroy(o.value)

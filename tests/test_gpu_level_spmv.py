@@ -86,6 +86,8 @@ def test_fp32_cycle_operator_bit_exact(gpu, oracle, nv):
     params = {"solver": {"method": "MergedPBiCGStab", "rel_tolerance": 1e-8, "max_iters": 5,
                          "gpu_index_compress": 2},
               "preconditioner": {"method": "MultiGrid", "mg_max_levels": 3,
+                                 "mg_coarsening_type": 8, "mg_interpolation_type": 6,
+                                 "mg_agg_num_levels": 0,
                                  "gpu_precond_f32": 1, "gpu_index_compress": 2},
               "pre_smoother": {"method": "Chebyshev"}, "post_smoother": {"method": "Chebyshev"}}
     _, _, _, S = solver_on(gpu, row, col, val, nv, params)
@@ -130,6 +132,8 @@ def test_bf16_cycle_operators_bit_exact(gpu, oracle, nv):
     params = {"solver": {"method": "MergedPBiCGStab", "rel_tolerance": 1e-8, "max_iters": 5,
                          "gpu_index_compress": 2},
               "preconditioner": {"method": "MultiGrid", "mg_max_levels": 3,
+                                 "mg_coarsening_type": 8, "mg_interpolation_type": 6,
+                                 "mg_agg_num_levels": 0,
                                  "gpu_precond_f32": 1, "gpu_index_compress": 2,
                                  "gpu_level_bf16": 2},
               "pre_smoother": {"method": "Chebyshev"}, "post_smoother": {"method": "Chebyshev"}}

@@ -403,3 +403,114 @@ def test_graph_fallback_keeps_zero_flag(gpu, method):
         assert x0.tobytes() == x1.tobytes()
     r = true_rel_res(row, col, val, results[1][-1][0], b, nv)
     assert r.max() < 1e-7
+
+
+@pytest.mark.parametrize("f32", [0, 1])
+def test_w_cycle(gpu, oracle, f32):
+    """mg_cycle = 2 (W-cycle, mg.inl:229-232) as the preconditioner, FP64 or
+    FP32, against the oracle bit for bit and XAMG's order to 1e-6."""
+    row, col, val = gpu.generate_diffusion(27, 14, 13, 12, 1.0, 1.0, 21)
+    sm = {"method": "Chebyshev", "polynomial_order": 2}
+    params = {"solver": {"method": "MergedPBiCGStab", "max_iters": 100, "rel_tolerance": 1e-8,
+                         "abs_tolerance": 0},
+              "preconditioner": dict(MG_BASE, method="MultiGrid", mg_cycle=2,
+                                     mg_coarse_matrix_size=20),
+              "pre_smoother": sm, "post_smoother": dict(sm),
+              "coarse_grid_solver": {"method": "Direct"}}
+    if f32:
+        params["solver"]["gpu_index_compress"] = 2
+        params["preconditioner"].update(gpu_precond_f32=1, gpu_index_compress=2)
+    st, S = check(gpu, oracle, row, col, val, 4, params, seed=2)
+    assert S.nlevels() >= 4
+
+
+@pytest.mark.parametrize("f32", [0, 1])
+def test_f_cycle_as_the_reference_runs_it(gpu, oracle, f32):
+    """mg_cycle = 1 (F-cycle, mg.inl:198,233-234). Its first visit of a level
+    skips pre-smoothing, and the prolongation then adds P x_H to whatever the
+    zero-flagged x holds from the previous cycle (blas2 Axpy accumulates into
+    the vector's memory). The reference built from its own sources does
+    exactly this (oracle pinned to it in tests/test_ref_pins.py), and on this
+    matrix the preconditioner it gives stalls the iteration. The GPU must
+    reproduce the same iterates bit for bit, solve after solve."""
+    row, col, val = gpu.generate_diffusion(27, 14, 13, 12, 1.0, 1.0, 21)
+    nv = 4
+    sm = {"method": "Chebyshev", "polynomial_order": 2}
+    params = {"solver": {"method": "MergedPBiCGStab", "max_iters": 30, "rel_tolerance": 1e-8,
+                         "abs_tolerance": 0},
+              "preconditioner": dict(MG_BASE, method="MultiGrid", mg_cycle=1,
+                                     mg_coarse_matrix_size=20),
+              "pre_smoother": sm, "post_smoother": dict(sm),
+              "coarse_grid_solver": {"method": "Direct"}}
+    if f32:
+        params["solver"]["gpu_index_compress"] = 2
+        params["preconditioner"].update(gpu_precond_f32=1, gpu_index_compress=2)
+    n = len(row) - 1
+    b = np.random.default_rng(1).uniform(-1, 1, n * nv)
+    M = gpu.Matrix(row, col, val)
+    X, B = gpu.Vector(n, nv, M.part), gpu.Vector(n, nv, M.part)
+    B.upload(b)
+    X.set(0.0)
+    S = gpu.Solver(M, gpu.Params(params), X, B)
+    sysm = oracle.System(nv)
+    sysm.set_params(params)
+    for lv in S.hierarchy():
+        sysm.add_level(*lv["A"], lv["min_eig"], lv["max_eig"])
+        if lv["P"] is not None:
+            sysm.add_interp(*lv["P"])
+    sysm.setup()
+    for _ in range(2):   # the second solve starts from the buffers the first left
+        X.set(0.0)
+        S.solve()
+        xg, sg = X.download(), S.stats()
+        oracle.set_reduction(1)
+        try:
+            xo, so = sysm.solve(b)
+        finally:
+            oracle.set_reduction(0)
+        assert sg["iters"] == so["iters"]
+        assert sg["conv"].tolist() == so["conv"].tolist()
+        assert xg.tobytes() == xo.tobytes()
+
+
+def test_max_levels_truncation(gpu, oracle):
+    """mg_max_levels stops the hierarchy early: the Direct coarse solve then
+    inverts a larger coarsest level (inverse.inl:31-106)."""
+    row, col, val = gpu.generate_diffusion(7, 18, 17, 16, 1.0, 1.0, 22)
+    params = {"solver": {"method": "PBiCGStab", "max_iters": 100, "rel_tolerance": 1e-8,
+                         "abs_tolerance": 0},
+              "preconditioner": dict(MG_BASE, method="MultiGrid", mg_max_levels=2),
+              "pre_smoother": {"method": "Jacobi"}, "post_smoother": {"method": "Jacobi"},
+              "coarse_grid_solver": {"method": "Direct"}}
+    st, S = check(gpu, oracle, row, col, val, 2, params, seed=3)
+    assert S.nlevels() == 2
+    assert S.level_info(1, 0)["nrows"] > 300
+
+
+@pytest.mark.parametrize("key,value", [("mg_coarsening_type", 10), ("mg_coarsening_type", 6),
+                                       ("mg_interpolation_type", 0),
+                                       ("mg_agg_num_levels", 2)])
+def test_unsupported_hierarchy_options_are_refused(gpu, key, value):
+    """The host setup implements PMIS with extended+i and no aggressive
+    levels; other choices (hypre_base.h:155-163) are refused with
+    XAMG_ERR_UNSUPPORTED instead of being replaced, also when given as a
+    per-level override."""
+    row, col, val = gpu.generate_cube(10, 10, 10)
+    n = len(row) - 1
+    for as_override in (False, True):
+        pre = dict(MG_BASE, method="MultiGrid")
+        overrides = None
+        if as_override:
+            overrides = {"preconditioner": {key: f"{value}@lev1"}}
+        else:
+            pre[key] = value
+        params = {"solver": {"method": "PBiCGStab", "max_iters": 10},
+                  "preconditioner": pre}
+        M = gpu.Matrix(row, col, val)
+        X, B = gpu.Vector(n, 1, M.part), gpu.Vector(n, 1, M.part)
+        X.set(0.0)
+        B.set(1.0)
+        with pytest.raises(gpu.XamgError) as e:
+            gpu.Solver(M, gpu.Params(params, overrides=overrides), X, B)
+        assert e.value.code == -8, (key, value, as_override)
+        assert key in gpu.last_error()

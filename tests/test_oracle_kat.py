@@ -288,3 +288,22 @@ def test_oracle_residual_drop_multi_rhs(oracle):
     A = sp.csr_matrix((val, col, row))
     r = b.reshape(-1, nv) - A @ x.reshape(-1, nv)
     assert (np.linalg.norm(r, axis=0) / np.linalg.norm(b.reshape(-1, nv), axis=0)).max() <= 1e-10
+
+
+def test_bf16_rounding_matches_torch(oracle):
+    """The oracle's BF16 rounding (round to nearest, ties to even) equals
+    torch's float32 -> bfloat16 conversion, ties and extremes included."""
+    import torch
+    rng = np.random.default_rng(17)
+    a = np.concatenate([
+        rng.standard_normal(100000).astype(np.float32) * np.float32(1e3),
+        (rng.standard_normal(1000) * 1e-39).astype(np.float32),        # subnormals
+        np.array([0.0, -0.0, np.inf, -np.inf, 3.4e38, -3.4e38, 1.0, 1.00390625,
+                  1.01171875, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -8], np.float32)])
+    # exact ties: low 16 bits = 0x8000 with either parity of the kept bit
+    u = rng.integers(0, 2 ** 31, 2000, dtype=np.uint32) & np.uint32(0x7F7F0000)
+    ties = ((u | np.uint32(0x8000))).view(np.float32)
+    a = np.concatenate([a, ties])
+    want = torch.from_numpy(a).to(torch.bfloat16).to(torch.float32).numpy()
+    got = oracle.round_bf16(a)
+    assert got.tobytes() == want.tobytes()
