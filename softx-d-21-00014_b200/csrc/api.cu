@@ -47,8 +47,8 @@ struct MatObj {
     HierCache hcache;  // host multigrid hierarchies built for this matrix
     // device copies keyed by the narrowing switch and the tuning switch
     std::map<int, std::unique_ptr<DCsr>> dev;
-    const DCsr *device(int narrow, bool tune) {
-        auto &p = dev[narrow * 2 + (tune ? 1 : 0)];
+    const DCsr *device(int narrow, int tune) {
+        auto &p = dev[narrow * 4 + tune];
         if (!p) {
             p.reset(new DCsr());
             upload_csr(h, *p, false, narrow, ctx().stream, tune);
@@ -516,7 +516,7 @@ static void build_solver(SolverObj &so, const Params &P, int nv) {
     XG_REQUIRE(m.constructed, XAMG_ERR_INVALID_ARG, "matrix not constructed");
     SolverCfg c = resolve_cfg(P.get("solver"), "solver");
     const int narrow = c.gpu_index_compress;
-    const DCsr *A = m.device(narrow, c.gpu_spmv_tune != 0);
+    const DCsr *A = m.device(narrow, c.gpu_spmv_tune);
     so.sh.reset(new SolverHierarchy());
     so.sh->build(P, m.h, A, nv, &m.hcache);
     so.nv = nv;

@@ -225,9 +225,10 @@ template void axpy_k<float>(float *, const float *, const double *, uint64_t, in
 // CSR upload with XAMG's narrowing (matrix_block::assemble, matrix.h:78-93:
 // hash from encode_hash, values converted to float when reduced).
 // ---------------------------------------------------------------------------
-void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s, bool tune,
+void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s, int tune,
                 bool bf16) {
-    d.tune_on = tune;
+    d.tune_on = tune != 0;
+    d.force_sell = tune == 2;
     d.bf16 = f32 && bf16;
     d.nrows = h.nrows;
     d.ncols = h.ncols;

@@ -240,7 +240,7 @@ struct Hsgs : public SolverBase {
             od.row[i + 1] = (uint32_t)od.col.size();
         }
         upload_csr(dg, Adiag, f32, cfg.gpu_index_compress, S());
-        upload_csr(od, Aoff, f32, cfg.gpu_index_compress, S(), cfg.gpu_spmv_tune != 0);
+        upload_csr(od, Aoff, f32, cfg.gpu_index_compress, S(), cfg.gpu_spmv_tune);
         upload(boff, off, S());
         if (f32)
             upload(d, inv_diag_f32(hA, false), S());
@@ -515,7 +515,7 @@ void MultiGrid::build(const HCsr &A0, const DCsr *A0dev, const Params &P, const 
                                                   : cfg.mg_reduced_precision != 0;
     full32 = (cfg.gpu_precond_f32 == 1) && role == "preconditioner";
     const int narrow = cfg.gpu_index_compress;
-    const bool tune = cfg.gpu_spmv_tune != 0;
+    const int tune = cfg.gpu_spmv_tune;
     L.clear();
     L.resize(nl);
     for (int l = 0; l < nl; ++l) {

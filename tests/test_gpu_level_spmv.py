@@ -60,17 +60,19 @@ def run_level_spmv(gpu, S, level, which, row, col, val, nv, f32, seed):
     return xh, y0, y.cpu().numpy(), ya.cpu().numpy()
 
 
-def krylov():
-    return {"solver": {"method": "MergedPBiCGStab", "rel_tolerance": 1e-8, "max_iters": 10},
+def krylov(tune=1):
+    return {"solver": {"method": "MergedPBiCGStab", "rel_tolerance": 1e-8, "max_iters": 10,
+                       "gpu_spmv_tune": tune},
             "preconditioner": {"method": "Jacobi"}}
 
 
 @pytest.mark.parametrize("nv", [1, 2, 4, 8, 16, 32])
 @pytest.mark.parametrize("n,far_from,diag_first", [(3001, 2400, False), (2000, 2000, True),
                                                    (257, 200, False), (1003, 1003, True)])
-def test_fp64_level_spmv_bit_exact(gpu, oracle, nv, n, far_from, diag_first):
+@pytest.mark.parametrize("tune", [1, 2])
+def test_fp64_level_spmv_bit_exact(gpu, oracle, nv, n, far_from, diag_first, tune):
     row, col, val = banded_plus_random(n, far_from, 9, seed=n + nv, diag_first=diag_first)
-    _, _, _, S = solver_on(gpu, row, col, val, nv, krylov())
+    _, _, _, S = solver_on(gpu, row, col, val, nv, krylov(tune))
     xh, y0, y, ya = run_level_spmv(gpu, S, 0, 0, row, col, val, nv, False, seed=nv)
     want = oracle.csr_ax_y(row, col, val, xh, nv)
     assert y.tobytes() == want.tobytes()
@@ -79,7 +81,8 @@ def test_fp64_level_spmv_bit_exact(gpu, oracle, nv, n, far_from, diag_first):
 
 
 @pytest.mark.parametrize("nv", [1, 4, 8, 32])
-def test_fp32_cycle_operator_bit_exact(gpu, oracle, nv):
+@pytest.mark.parametrize("tune", [1, 2])
+def test_fp32_cycle_operator_bit_exact(gpu, oracle, nv, tune):
     """Level 0 of an FP32 multigrid preconditioner (gpu_precond_f32 = 1),
     with 2-byte relative columns, on a 27-point FE matrix."""
     row, col, val = gpu.generate_diffusion(27, 14, 13, 12, 1.0, 1.0, 3)
@@ -87,7 +90,7 @@ def test_fp32_cycle_operator_bit_exact(gpu, oracle, nv):
                          "gpu_index_compress": 2},
               "preconditioner": {"method": "MultiGrid", "mg_max_levels": 3,
                                  "mg_coarsening_type": 8, "mg_interpolation_type": 6,
-                                 "mg_agg_num_levels": 0,
+                                 "mg_agg_num_levels": 0, "gpu_spmv_tune": tune,
                                  "gpu_precond_f32": 1, "gpu_index_compress": 2},
               "pre_smoother": {"method": "Chebyshev"}, "post_smoother": {"method": "Chebyshev"}}
     _, _, _, S = solver_on(gpu, row, col, val, nv, params)
@@ -100,7 +103,8 @@ def test_fp32_cycle_operator_bit_exact(gpu, oracle, nv):
 
 
 @pytest.mark.parametrize("nv", [1, 8, 32])
-def test_fp64_27pt_diag_first(gpu, oracle, nv):
+@pytest.mark.parametrize("tune", [1, 2])
+def test_fp64_27pt_diag_first(gpu, oracle, nv, tune):
     """27-point FE rows stored diagonal first (hypre's order)."""
     row, col, val = gpu.generate_diffusion(27, 13, 12, 11, 1.0, 1.0, 5)
     col, val = col.copy(), val.copy()
@@ -109,7 +113,7 @@ def test_fp64_27pt_diag_first(gpu, oracle, nv):
         d = a + int(np.nonzero(col[a:b] == i)[0][0])
         order = [d] + [j for j in range(a, b) if j != d]
         col[a:b], val[a:b] = col[order], val[order]
-    _, _, _, S = solver_on(gpu, row, col, val, nv, krylov())
+    _, _, _, S = solver_on(gpu, row, col, val, nv, krylov(tune))
     xh, y0, y, ya = run_level_spmv(gpu, S, 0, 0, row, col, val, nv, False, seed=nv)
     assert y.tobytes() == oracle.csr_ax_y(row, col, val, xh, nv).tobytes()
     assert ya.tobytes() == oracle.csr_ax_y(row, col, val, xh, nv, axpy_y=y0).tobytes()
@@ -124,7 +128,8 @@ def bf16_round(v):
 
 
 @pytest.mark.parametrize("nv", [1, 8, 32])
-def test_bf16_cycle_operators_bit_exact(gpu, oracle, nv):
+@pytest.mark.parametrize("tune", [1, 2])
+def test_bf16_cycle_operators_bit_exact(gpu, oracle, nv, tune):
     """gpu_level_bf16 = 2: the two finest FP32 cycle operators store BF16
     values and compute in float. Their SpMVs must equal the oracle's float
     row sums over the BF16-rounded values bit for bit."""
@@ -133,7 +138,7 @@ def test_bf16_cycle_operators_bit_exact(gpu, oracle, nv):
                          "gpu_index_compress": 2},
               "preconditioner": {"method": "MultiGrid", "mg_max_levels": 3,
                                  "mg_coarsening_type": 8, "mg_interpolation_type": 6,
-                                 "mg_agg_num_levels": 0,
+                                 "mg_agg_num_levels": 0, "gpu_spmv_tune": tune,
                                  "gpu_precond_f32": 1, "gpu_index_compress": 2,
                                  "gpu_level_bf16": 2},
               "pre_smoother": {"method": "Chebyshev"}, "post_smoother": {"method": "Chebyshev"}}

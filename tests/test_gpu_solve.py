@@ -335,15 +335,17 @@ def test_rbicgstab_with_amg(gpu, oracle, method, f32):
 @pytest.mark.parametrize("stencil,edge,nv,f32", [(27, 14, 8, True), (27, 12, 4, False),
                                                  (7, 20, 16, True), (7, 18, 32, False)])
 def test_autotuned_spmv_same_results(gpu, stencil, edge, nv, f32):
-    """The SpMV autotuner (gpu_spmv_tune) only picks launch shapes: a solve
-    with it equals the solve without it bit for bit, and it has recorded a
-    choice for the matrices the preconditioner's SpMVs ran on."""
+    """The SpMV autotuner (gpu_spmv_tune = 1) only picks launch shapes, the
+    sliced kernel among them (gpu_spmv_tune = 2 forces it for every SpMV
+    without dot products): a solve with either equals the solve without
+    tuning bit for bit, and the choice is recorded for the matrices the
+    preconditioner's SpMVs ran on."""
     row, col, val = gpu.generate_diffusion(stencil, edge, edge, edge, 1.0, 1.0, 4)
     n = len(row) - 1
     b = np.random.default_rng(9).uniform(-1, 1, n * nv)
     sm = {"method": "Chebyshev", "polynomial_order": 2}
     out = {}
-    for tune in (0, 1):
+    for tune in (0, 1, 2):
         params = {"solver": {"method": "MergedPBiCGStab", "max_iters": 100,
                              "rel_tolerance": 1e-8, "abs_tolerance": 0, "gpu_spmv_tune": tune},
                   "preconditioner": dict(MG_BASE, method="MultiGrid",
@@ -354,8 +356,11 @@ def test_autotuned_spmv_same_results(gpu, stencil, edge, nv, f32):
         out[tune] = (x, st)
         codes = S.level_tuned(1, 3)
         assert (codes.any()) == bool(tune)
-    assert out[0][0].tobytes() == out[1][0].tobytes()
-    assert out[0][1]["iters"] == out[1][1]["iters"]
+        if tune == 2:   # every SpMV without dot products on the sliced kernel
+            assert set(codes[codes != 0].tolist()) == {20}
+    for tune in (1, 2):
+        assert out[0][0].tobytes() == out[tune][0].tobytes()
+        assert out[0][1]["iters"] == out[tune][1]["iters"]
 
 
 @pytest.mark.parametrize("method", ["PCG", "MergedRBiCGStab"])
@@ -514,3 +519,42 @@ def test_unsupported_hierarchy_options_are_refused(gpu, key, value):
             gpu.Solver(M, gpu.Params(params, overrides=overrides), X, B)
         assert e.value.code == -8, (key, value, as_override)
         assert key in gpu.last_error()
+
+
+@pytest.mark.parametrize("case", ["config1", "amg27"])
+def test_gpu_against_the_reference_itself(gpu, case):
+    """The GPU solve against XAMG's own solve phase built from the reference
+    sources (oracle/_ref, one rank) on the same inputs and hierarchy: the
+    solutions agree to 1e-6 relative and both converge."""
+    import ref_capi
+    if not ref_capi.available(1):
+        pytest.skip("reference not built here")
+    if case == "config1":
+        row, col, val = gpu.generate_cube(32, 32, 32)
+        nv = 1
+        params = {"solver": {"method": "MergedPBiCGStab", "max_iters": 1000,
+                             "rel_tolerance": 1e-8, "abs_tolerance": 0},
+                  "preconditioner": {"method": "Jacobi"}}
+    else:
+        row, col, val = gpu.generate_diffusion(27, 24, 24, 24, 1.0, 1.0, 0)
+        nv = 8
+        sm = {"method": "Chebyshev", "polynomial_order": 2}
+        params = {"solver": {"method": "MergedPBiCGStab", "max_iters": 200,
+                             "rel_tolerance": 1e-8, "abs_tolerance": 0},
+                  "preconditioner": dict(MG_BASE, method="MultiGrid"),
+                  "pre_smoother": sm, "post_smoother": dict(sm),
+                  "coarse_grid_solver": {"method": "Direct"}}
+    n = len(row) - 1
+    b = np.random.default_rng(77).uniform(-1, 1, n * nv)
+    xg, sg, S = gpu_solve(gpu, row, col, val, nv, params, b)
+    H = S.hierarchy() if case != "config1" else None
+    R = ref_capi.Solve(row, col, val, nv, params, hierarchy=H)
+    try:
+        xr, conv = R.solve(b)
+    finally:
+        R.close()
+    assert conv.all() and sg["conv"].all()
+    X, Xr = xg.reshape(-1, nv), xr.reshape(-1, nv)
+    err = np.linalg.norm(X - Xr, axis=0) / np.linalg.norm(Xr, axis=0)
+    assert err.max() <= 1e-6, err
+    assert true_rel_res(row, col, val, xg, b, nv).max() <= 1e-8 * 1.5
