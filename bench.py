@@ -191,6 +191,8 @@ def run_ours(args, w):
     for name, reduced in (("fp64", False), ("chosen", True)):
         if w["smoother"] is None and reduced:
             continue
+        if args.solves_only and args.solves_only != name:
+            continue
         solvers[name] = X.Solver(M, X.Params(params_for(w, reduced)), xv, bv)
     setup_s = time.time() - t0
     chosen = "chosen" if "chosen" in solvers else "fp64"
@@ -220,6 +222,16 @@ def run_ours(args, w):
         barrier(ws)
         ms = ev0.elapsed_time(ev1)
         return max_over_ranks(ms, ws), X.kernel_launches() - k0, xh_pin.numpy().copy()
+
+    if args.solves_only:
+        # profiling aid: W + K solves of one arm and nothing else
+        S = solvers[args.solves_only]
+        for _ in range(args.warmup):
+            xv.set(0.0)
+            S.solve()
+        ms, launches, _ = timed(S, args.steps)
+        return {"arm": args.solves_only, "ms_per_rhs": ms / (args.steps * nv),
+                "iters": S.stats()["iters"], "launches_per_solve": launches / args.steps}
 
     if args.roofline_only:
         return roofline(X, torch, stream, solvers[chosen], n, nv, args,
@@ -677,6 +689,9 @@ def main():
     ap.add_argument("--workload", default="amg27", choices=sorted(WORKLOADS))
     ap.add_argument("--grid", type=int, default=None, help="override the grid edge")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--solves-only", choices=["fp64", "chosen"], default=None,
+                    help="set up one arm, then only its warm-up and timed solves: the command "
+                         "to profile that arm's launches")
     ap.add_argument("--roofline-only", action="store_true",
                     help="set up, then time only the level-0 SpMV (--steps launches): "
                          "the command to profile that kernel")

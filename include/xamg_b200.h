@@ -251,6 +251,13 @@ int XAMG_b200_vector_device_ptr(size_t vid, void **ptr);
  * the solve call. */
 int XAMG_b200_wait_selftest(double seconds, int *timed_out);
 
+/* Exercises the bounded grid barrier of the persistent BiCGStab launch (no
+ * counterpart): four blocks wait at a barrier that expects a fifth, each wait
+ * gives up after `seconds` (at most 1) and raises the timeout flag; on return
+ * *timed_out is 1 and the GPU context is still usable. The persistent solve
+ * waits at most 1 s at each barrier and reports XAMG_ERR_TIMEOUT. */
+int XAMG_b200_grid_selftest(double seconds, int *timed_out);
+
 /* Solves `count` independent systems together: entry i is
  * XAMG_solver_solve2(nv[i], xids[i], bids[i], sids[i]) (xamg_c_api.h:112),
  * with the same results bit for bit, but every system runs on a stream and

@@ -1097,4 +1097,21 @@ int XAMG_b200_wait_selftest(double seconds, int *timed_out) {
     });
 }
 
+int XAMG_b200_grid_selftest(double seconds, int *timed_out) {
+    return guarded([&] {
+        XG_REQUIRE(timed_out && seconds > 0 && seconds <= 1.0, XAMG_ERR_INVALID_ARG,
+                   "seconds must be in (0, 1]");
+        Ctx &c = ctx();
+        *timed_out = 0;
+        DevBuf cg(2 * sizeof(unsigned));
+        ops::grid_selftest(cg.as<unsigned>(), c.red().flag, (uint64_t)(seconds * 1e9), c.stream);
+        try {
+            c.check_flags();
+        } catch (const Error &e) {
+            if (e.code != XAMG_ERR_TIMEOUT) throw;
+            *timed_out = 1;
+        }
+    });
+}
+
 }  // extern "C"

@@ -528,9 +528,10 @@ __global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
 // --- sliced SpMV (SELL copy of the matrix, SpMVs without dot products) ------
 // A warp walks one unit of H = 32 / G consecutive rows (G = NV / VK threads a
 // row): at step j it reads the j-th entries of its H rows as one contiguous
-// load (no staging, no block barrier), gathers x for them and accumulates
-// each row over its own entries in CSR order, as k_spmv does, so every
-// result is the same bit for bit. A block takes chunks of `chunk`
+// load (no staging, no block barrier; the next steps' entries are loaded
+// while this step's x gathers run), gathers x for them and accumulates each
+// row over its own entries in CSR order with separately rounded multiplies
+// and adds, as k_spmv does, so every result is the same bit for bit. A block takes chunks of `chunk`
 // consecutive units (its warps interleaved over the chunk, so that the warps
 // sharing an SM's L1 work on neighbouring rows); the grid is one wave.
 template <typename I, typename V>
@@ -576,29 +577,28 @@ __device__ __forceinline__ __nv_bfloat16 ld_na(const __nv_bfloat16 *p) {
     return __ushort_as_bfloat16(ld_na((const uint16_t *)p));
 }
 
-// y0 += x0 * a, y1 += x1 * a as two float lanes of one packed multiply and
-// one packed add (sm_100 f32x2): each lane is rounded exactly as one
-// __fmul_rn followed by one __fadd_rn.
-__device__ __forceinline__ void mac2(float &y0, float &y1, float x0, float x1, float a) {
-    asm("{\n\t.reg .b64 yy, xx, aa;\n\t"
-        "mov.b64 yy, {%0, %1};\n\t"
-        "mov.b64 xx, {%2, %3};\n\t"
-        "mov.b64 aa, {%4, %4};\n\t"
-        "mul.rn.f32x2 xx, xx, aa;\n\t"
-        "add.rn.f32x2 yy, yy, xx;\n\t"
-        "mov.b64 {%0, %1}, yy;\n\t}"
-        : "+f"(y0), "+f"(y1)
-        : "f"(x0), "f"(x1), "f"(a));
-}
-
-template <typename F, typename FX, int VK>
-__device__ __forceinline__ void mac_row(F (&y)[VK], const FX (&xv)[VK], F a) {
-    if constexpr (std::is_same<F, float>::value && std::is_same<FX, float>::value && VK % 2 == 0) {
+// One unit's entries j .. j+P-1 of row q (those below len), loaded ahead of
+// their use.
+template <typename I, typename V, int H, int P, bool PACKED>
+__device__ __forceinline__ void sell_load(I (&cc)[P], V (&vv)[P], const uint32_t *pk, const I *col,
+                                          const V *val, uint32_t base, uint32_t j, uint32_t len,
+                                          int q) {
 #pragma unroll
-        for (int v = 0; v < VK; v += 2) mac2(y[v], y[v + 1], xv[v], xv[v + 1], a);
-    } else {
-#pragma unroll
-        for (int v = 0; v < VK; ++v) y[v] = add(y[v], mul((F)xv[v], a));
+    for (int p = 0; p < P; ++p) {
+        if (j + p < len) {
+            const uint32_t e = base + (j + p) * H + q;
+            if constexpr (PACKED) {
+                const uint32_t w = ld_na(pk + e);
+                cc[p] = (I)(uint16_t)(w & 0xffffu);
+                if constexpr (std::is_same<V, __nv_bfloat16>::value)
+                    vv[p] = __ushort_as_bfloat16((unsigned short)(w >> 16));
+                else
+                    vv[p] = (V)(uint16_t)(w >> 16);
+            } else {
+                cc[p] = ld_na(col + e);
+                vv[p] = ld_na(val + e);
+            }
+        }
     }
 }
 
@@ -629,33 +629,29 @@ __global__ void __launch_bounds__(256, 4)
             F y[VK];
 #pragma unroll
             for (int v = 0; v < VK; ++v) y[v] = live ? epi.init(i, k0 + v) : F(0);
+            // the next P entries are in flight while this step's x gathers
+            // and sums run
+            I cc[P], cn[P];
+            V vv[P], vn[P];
+            sell_load<I, V, H, P, PACKED>(cc, vv, pk, col, val, base, 0, len, q);
             for (uint32_t j = 0; j < width; j += P) {
-                I cc[P];
-                V vv[P];
-#pragma unroll
-                for (int p = 0; p < P; ++p) {
-                    if (j + p < len) {
-                        const uint32_t e = base + (j + p) * H + q;
-                        if constexpr (PACKED) {
-                            const uint32_t w = ld_na(pk + e);
-                            cc[p] = (I)(uint16_t)(w & 0xffffu);
-                            if constexpr (std::is_same<V, __nv_bfloat16>::value)
-                                vv[p] = __ushort_as_bfloat16((unsigned short)(w >> 16));
-                            else
-                                vv[p] = (V)(uint16_t)(w >> 16);
-                        } else {
-                            cc[p] = ld_na(col + e);
-                            vv[p] = ld_na(val + e);
-                        }
-                    }
-                }
                 FX xv[P][VK];
 #pragma unroll
                 for (int p = 0; p < P; ++p)
                     if (j + p < len) ld_x<FX, VK>(x + col_at<I>(cc[p], i) * NV + k0, xv[p]);
+                sell_load<I, V, H, P, PACKED>(cn, vn, pk, col, val, base, j + P, len, q);
 #pragma unroll
                 for (int p = 0; p < P; ++p)
-                    if (j + p < len) mac_row<F, FX, VK>(y, xv[p], val_as<F, V>(vv[p]));
+                    if (j + p < len) {
+                        const F a = val_as<F, V>(vv[p]);
+#pragma unroll
+                        for (int v = 0; v < VK; ++v) y[v] = add(y[v], mul((F)xv[p][v], a));
+                    }
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                    cc[p] = cn[p];
+                    vv[p] = vn[p];
+                }
             }
             if (live) {
 #pragma unroll
@@ -1434,6 +1430,244 @@ __global__ void __launch_bounds__(DT)
     }
     if (i < n) y[i * NV + k] = acc;
 }
+
+// --- persistent preconditioned BiCGStab ----------------------------------------
+// Grid barrier with a bounded wait: every block of a cooperative launch
+// arrives; the last one opens the next round. A block whose wait passes
+// limit_ns raises the timeout flag (read by the host as XAMG_ERR_TIMEOUT)
+// and returns false, and the kernel then ends; the other blocks' next waits
+// run out the same way, so no block waits without bound.
+struct GridSync {
+    unsigned *count;  // arrivals in the current round (zero between rounds)
+    unsigned *gen;    // rounds completed
+    unsigned *flag;   // bit 0: a wait ran out
+    uint64_t limit_ns;
+};
+__device__ __forceinline__ bool grid_sync(const GridSync &g, unsigned expected) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        const unsigned round = *(volatile unsigned *)g.gen;
+        __threadfence();
+        if (atomicAdd(g.count, 1u) == expected - 1) {
+            *(volatile unsigned *)g.count = 0u;
+            __threadfence();
+            atomicAdd(g.gen, 1u);
+        } else {
+            const uint64_t t0 = global_ns();
+            for (uint32_t it = 0; *(volatile unsigned *)g.gen == round; ++it) {
+                if (global_ns() - t0 > g.limit_ns || it == 0xffffffffu) {
+                    atomicOr(g.flag, 1u);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// The last step of the canonical reduction run by every block for itself
+// (the same sums, in the same order, as canon_final's last block), with the
+// finaliser writing the block's own copy of the scalar block: no block
+// depends on another's finaliser.
+template <int NV, int NRED, class Fin>
+__device__ __forceinline__ void canon_final_local(const double *part, uint32_t B, const Fin &fin) {
+    __shared__ double sums[NV * NRED];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int o = warp; o < NV * NRED; o += CT / 32) {
+        double a = 0.0;
+        for (unsigned bb = lane; bb < B; bb += 32) a = add(a, ld_cg(&part[(size_t)bb * NV * NRED + o]));
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) a = add(a, shfl_xor(a, off));
+        if (lane == 0) sums[o] = a;
+    }
+    __syncthreads();
+    for (int kk = threadIdx.x; kk < NV; kk += CT) fin(kk, &sums[kk * NRED]);
+    __syncthreads();
+}
+
+struct PersistArgs {
+    double *x, *r0, *r, *p, *v, *s, *t, *pa, *sa, *tmp;
+    const double *d;   // Jacobi inverse diagonal; null: no preconditioner (pa = p, sa = s)
+    double relax;
+    int sweeps;        // Jacobi sweeps (max_iters of the preconditioner list)
+    double *sc;        // the solver's scalar block: read at the start, written at the end
+    double *out;       // [3][32]: abs_res, rel_res, conv (0/1); [96]: iterations
+    int max_iters, check;
+    float abs_tol, rel_tol;
+    RedArgs ra;        // partial sums: two halves used in turn
+    GridSync gs;
+};
+
+// merged_pbicgstab.inl:44-225 after its start (r0, rho0, p = r = r0 and the
+// first test, done by Krylov::begin/started): every iteration, its
+// convergence test (solver.h:173-241 with float32 tolerances) and the final
+// x update in one cooperative launch of B = canon_blocks(n, NV) blocks of 256
+// threads, block b being canonical block b (grid barriers between the
+// steps). Each step applies the same element operations, row sums and
+// canonical reductions as the separate kernels of Krylov::step_tail,
+// step_body and stepped, so the iterates are the same bit for bit.
+template <int NV, typename I>
+__global__ void __launch_bounds__(CT, 1) k_pbicgstab_persist(CsrArgs<double> A, PersistArgs P) {
+    constexpr int R = CT / NV;
+    __shared__ double SCS[SC_COUNT * SC_STRIDE];
+    __shared__ double st_abs[NV], st_rel[NV];
+    __shared__ int st_conv[NV];
+    __shared__ int go;
+    const uint32_t B = gridDim.x;
+    const uint64_t n = A.n;
+    const uint64_t ntiles = (n + R - 1) / R;
+    const int rt = threadIdx.x / NV, kk = threadIdx.x % NV;
+    const uint32_t *__restrict__ row = A.row;
+    const I *__restrict__ col = (const I *)A.col;
+    const double *__restrict__ val = A.val;
+    for (int o = threadIdx.x; o < SC_COUNT * SC_STRIDE; o += CT) SCS[o] = P.sc[o];
+    for (int o = threadIdx.x; o < NV; o += CT) {
+        st_abs[o] = 0.0;
+        st_rel[o] = 0.0;
+        st_conv[o] = 0;
+    }
+    __syncthreads();
+    uint32_t half = 0;  // which half of the partial-sum buffer this reduction writes
+    const size_t HALF = (size_t)B * NV * 4;
+    auto part = [&]() { return (double *)P.ra.part + (size_t)half * HALF; };
+    // every (row, right-hand side) this thread owns: canonical thread
+    // threadIdx.x of canonical block blockIdx.x, tiles in order
+    auto each = [&](auto &&fn) {
+        for (uint64_t tile = blockIdx.x; tile < ntiles; tile += B) {
+            const uint64_t i = tile * R + rt;
+            if (i < n) fn(i, (uint64_t)i * NV + kk);
+        }
+    };
+    // x written by other blocks in this launch: read through L2 (ld.cg), not
+    // from a possibly stale L1 line
+    auto rowsum = [&](const double *xv, uint64_t i) {
+        double y = 0.0;
+        for (uint32_t j = __ldg(&row[i]); j < __ldg(&row[i + 1]); ++j)
+            y = add(y, mul(ld_cg(&xv[col_at<I>(__ldg(&col[j]), i) * NV + kk]), __ldg(&val[j])));
+        return y;
+    };
+    auto sync = [&]() { return grid_sync(P.gs, B); };
+    auto reduce = [&](auto &acc, auto &&fin) {
+        constexpr int NR = sizeof(acc[0]) / sizeof(double);
+        canon_partial<double, NV, NR, 1>(acc, RedArgs{part(), nullptr, nullptr}, blockIdx.x);
+        if (!sync()) return false;
+        canon_final_local<NV, NR>(part(), B, fin);
+        half ^= 1u;
+        return true;
+    };
+    // out = M^-1 in: Jacobi sweeps from zero (jacobi.inl:113-119,
+    // blas_merged_jacobi.inl), the last landing in out; without a
+    // preconditioner pa/sa are p/s themselves
+    auto precond = [&](double *out, const double *in) {
+        if (!P.d) return true;
+        const int m = P.sweeps < 1 ? 1 : P.sweeps;
+        auto tgt = [&](int j) { return ((m - j) % 2 == 0) ? out : P.tmp; };
+        double *cur = tgt(1);
+        const OpJacobiZero<double> jz{cur, in, P.d, P.relax, NV};
+        each([&](uint64_t, uint64_t e) { jz(e); });
+        for (int j = 2; j <= m; ++j) {
+            if (!sync()) return false;
+            double *o = tgt(j);
+            const EJacobi<double, NV> ej{{}, o, cur, in, P.d, P.relax};
+            double none[1];
+            each([&](uint64_t i, uint64_t) { ej.store(i, kk, rowsum(cur, i), none); });
+            cur = o;
+        }
+        return true;
+    };
+    int it = 0;
+    bool tail = false, done = false, ok = true;
+    const EGroup4<NV, true> g4{P.s, P.t, P.r0, P.r, P.x, P.pa, P.sa, SCS};
+    const OpPUpdate pu{P.p, P.r, P.v, SCS, NV};
+    auto do_tail = [&]() {
+        double acc[1][1] = {{0.0}};
+        each([&](uint64_t i, uint64_t) { g4.elem(i, kk, acc[0]); });
+        if (!reduce(acc, g4)) return false;
+        each([&](uint64_t, uint64_t e) { pu(e); });
+        return true;
+    };
+    while (ok) {
+        ++it;
+        if (tail && !(ok = do_tail())) break;
+        if (!(ok = precond(P.pa, P.p))) break;
+        if (!(ok = sync())) break;
+        {   // v = A p_; alpha = rho / (v, r0)
+            const EDotAlpha<NV> ea{P.v, P.r0, SCS};
+            double acc[1][1] = {{0.0}};
+            each([&](uint64_t i, uint64_t) { ea.store(i, kk, rowsum(P.pa, i), acc[0]); });
+            if (!(ok = reduce(acc, ea))) break;
+        }
+        {   // s = r - alpha v
+            const OpSUpdate su{P.s, P.r, P.v, SCS, NV};
+            each([&](uint64_t, uint64_t e) { su(e); });
+        }
+        if (!(ok = precond(P.sa, P.s))) break;
+        if (!(ok = sync())) break;
+        {   // t = A s_; omega, res
+            const EDot3<NV> e3{P.t, P.s, SCS};
+            double acc[1][3] = {{0.0, 0.0, 0.0}};
+            each([&](uint64_t i, uint64_t) { e3.store(i, kk, rowsum(P.sa, i), acc[0]); });
+            if (!(ok = reduce(acc, e3))) break;
+        }
+        // convergence test (host_converged): every block decides alike
+        if (threadIdx.x == 0) {
+            bool flag = P.check != 0;
+            if (flag) {
+                for (int k2 = 0; k2 < NV; ++k2) {
+                    if (SCS[SC_ICONV * SC_STRIDE + k2] != 0.0) {
+                        const double a = sqrt(SCS[SC_RES * SC_STRIDE + k2]);
+                        const double rr = a / sqrt(SCS[SC_RHO0 * SC_STRIDE + k2]);
+                        if ((a > (double)P.abs_tol) && (rr > (double)P.rel_tol)) {
+                            flag = false;
+                        } else if (!st_conv[k2]) {
+                            st_abs[k2] = a;
+                            st_rel[k2] = rr;
+                            st_conv[k2] = 1;
+                        }
+                    }
+                }
+                if (!flag)
+                    for (int k2 = 0; k2 < NV; ++k2)
+                        SCS[SC_ICONV * SC_STRIDE + k2] =
+                            mul(SCS[SC_ICONV * SC_STRIDE + k2], (double)(!st_conv[k2]));
+            }
+            go = flag ? 0 : (it >= P.max_iters ? 1 : 2);
+        }
+        __syncthreads();
+        if (go == 0) {   // converged: x = alpha_c p_ + omega_c s_ + x
+            const OpXUpdate xu{P.x, P.pa, P.sa, SCS, NV};
+            each([&](uint64_t, uint64_t e) { xu(e); });
+            done = true;
+            break;
+        }
+        tail = true;
+        if (go == 1) {   // max_iters reached: the pending rest of the iteration
+            ok = do_tail();
+            done = ok;
+            break;
+        }
+    }
+    if (blockIdx.x == 0 && done) {
+        for (int o = threadIdx.x; o < SC_COUNT * SC_STRIDE; o += CT) P.sc[o] = SCS[o];
+        for (int o = threadIdx.x; o < NV; o += CT) {
+            P.out[o] = st_abs[o];
+            P.out[32 + o] = st_rel[o];
+            P.out[64 + o] = (double)st_conv[o];
+        }
+        if (threadIdx.x == 0) P.out[96] = (double)it;
+    }
+}
+
+// Waits at a grid barrier that one more block than the grid must reach:
+// every wait runs out after limit_ns and raises the timeout flag (the
+// barrier's bounded wait, exercised without a fault).
+static __global__ void k_grid_selftest(GridSync g) { (void)grid_sync(g, gridDim.x + 1); }
 
 }  // namespace k
 }  // namespace xg

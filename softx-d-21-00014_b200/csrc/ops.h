@@ -14,6 +14,14 @@ namespace ops {
 // Launches a wait that must run out after limit_ns (raises the timeout flag).
 void wait_selftest(uint64_t limit_ns, cudaStream_t s);
 
+// The persistent preconditioned BiCGStab (csrc/persist.cu): whether the
+// matrix's canonical blocks can all be resident at once, and the launch.
+bool pbicgstab_persist_fits(const DCsr &A, int nv);
+void pbicgstab_persist(const DCsr &A, const k::PersistArgs &P, int nv, cudaStream_t s);
+// A grid barrier that one block never reaches: its waits run out after
+// limit_ns and raise *flag.
+void grid_selftest(unsigned *count_gen, unsigned *flag, uint64_t limit_ns, cudaStream_t s);
+
 // Resolves the fixed scratch array of XAMG_b200_dot_noalloc and loads its
 // kernels on the current device (csrc/noalloc.cu); returns an XAMG status.
 int noalloc_prepare_current_device();

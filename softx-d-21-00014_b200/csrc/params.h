@@ -85,6 +85,7 @@ struct SolverCfg {
     int gpu_spmv_tune = 1;      // SpMV launch shapes picked by measurement
     int gpu_level_bf16 = 0;     // finest FP32 cycle levels whose matrix values are BF16
     int gpu_seed = 0;           // seed of the host setup's random choices
+    int gpu_persistent = 1;     // eligible BiCGStab solves in one cooperative launch
 };
 
 SolverCfg resolve_cfg(const PList &l, const std::string &role);

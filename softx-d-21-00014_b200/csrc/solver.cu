@@ -929,6 +929,10 @@ void Krylov::solve(DVec &x, DVec &b, const std::vector<double> &conv) {
     begin(x, b, conv);
     XG_CUDA(cudaStreamSynchronize(S()));
     if (started()) return;
+    if (persistent_ok()) {
+        run_persistent(x);
+        return;
+    }
     while (true) {
         step();
         XG_CUDA(cudaStreamSynchronize(S()));
@@ -970,6 +974,66 @@ void Krylov::begin(DVec &x, DVec &b, const std::vector<double> &conv) {
 bool Krylov::started() {
     take_scalars(run_.rho0.data(), NV);
     return check(run_.rho0.data(), run_.rho0.data(), run_.iconv);
+}
+
+// gpu_persistent (default 1): the preconditioned forms (PBiCGStab,
+// MergedPBiCGStab) with no preconditioner or a Jacobi preconditioner without
+// its own convergence test run every iteration in one cooperative launch
+// when the matrix's canonical blocks fit the GPU at once (small and
+// mid-sized systems; the 32^3 Poisson system has 128); printing residuals
+// (convergence_info) keeps the host loop.
+bool Krylov::persistent_ok() const {
+    if (!cfg.gpu_persistent || !precond_form || cfg.convergence_info || f32) return false;
+    if (M) {
+        auto *j = dynamic_cast<const Jacobi<double> *>(M.get());
+        if (!j || j->cfg.convergence_check || j->f32) return false;
+    }
+    return ops::pbicgstab_persist_fits(*A, NV);
+}
+
+void Krylov::run_persistent(DVec &x) {
+    cudaStream_t s = S();
+    auto *jac = M ? dynamic_cast<Jacobi<double> *>(M.get()) : nullptr;
+    if (!psync.bytes) psync.alloc(2 * sizeof(unsigned));
+    if (!pout.bytes) pout.alloc(128 * sizeof(double));
+    XG_CUDA(cudaMemsetAsync(psync.p, 0, psync.bytes, s));
+    const k::RedArgs ra = ctx().red();
+    k::PersistArgs P{};
+    P.x = x.p<double>();
+    P.r0 = buf[0].p<double>();
+    P.r = buf[1].p<double>();
+    P.p = buf[2].p<double>();
+    P.v = buf[3].p<double>();
+    P.s = buf[4].p<double>();
+    P.t = buf[5].p<double>();
+    P.pa = M ? buf[6].p<double>() : P.p;
+    P.sa = M ? buf[7].p<double>() : P.s;
+    P.tmp = jac ? jac->buf[1].p<double>() : nullptr;
+    P.d = jac ? jac->d.as<double>() : nullptr;
+    P.relax = jac ? (double)jac->cfg.relax : 0.0;
+    P.sweeps = jac ? std::max(1, jac->cfg.max_iters) : 0;
+    P.sc = sc.as<double>();
+    P.out = pout.as<double>();
+    P.max_iters = cfg.max_iters;
+    P.check = cfg.convergence_check;
+    P.abs_tol = cfg.abs_tol;
+    P.rel_tol = cfg.rel_tol;
+    P.ra = ra;
+    P.gs = k::GridSync{psync.as<unsigned>(), psync.as<unsigned>() + 1, ra.flag, 1000000000ull};
+    ops::pbicgstab_persist(*A, P, NV, s);
+    double out[97];
+    XG_CUDA(cudaMemcpyAsync(out, pout.p, sizeof(out), cudaMemcpyDeviceToHost, s));
+    ctx().check_flags();  // synchronises; XAMG_ERR_TIMEOUT if a grid wait ran out
+    st.iters = (int)out[96];
+    for (int k = 0; k < NV; ++k)
+        if (out[64 + k] != 0.0) {
+            st.conv[k] = 1;
+            st.abs_res[k] = out[k];
+            st.rel_res[k] = out[32 + k];
+        }
+    for (int i = 1; i < 8; ++i) buf[i].zero = false;
+    x.zero = false;
+    x.init = true;
 }
 
 // The step graph for key; past 32 keys (many solution vectors) the graphs

@@ -129,6 +129,10 @@ class Krylov : public SolverBase {
     void upload_iconv(const std::vector<double> &iconv);
     void step_body();
     void step_tail();
+    // the whole iteration in one cooperative launch (k_pbicgstab_persist)
+    bool persistent_ok() const;
+    void run_persistent(DVec &x);
+    DevBuf psync, pout;  // grid barrier counters; the launch's statistics
     MGraph &step_graph(const std::tuple<int, bool, const void *> &key);
     void run_graphed(MGraph &g, DVec *x, const std::function<void()> &body);
     // per (out, in, in.zero, lane): a graph's kernels carry its lane's scratch

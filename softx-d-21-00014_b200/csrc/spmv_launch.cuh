@@ -188,13 +188,16 @@ static const DSell *sell_of(const DCsr &A, int H, cudaStream_t s) {
 // The sliced kernel: 256-thread blocks, a wave of them, chunks of `chunk`
 // units a block.
 constexpr uint32_t SELL_CHUNKS[3] = {8, 64, 512};
-constexpr int SELL_P = 4;  // entries whose loads a warp issues together
+// entries whose loads a warp issues together (fewer for FP64, within 64
+// registers a thread)
+template <typename FX>
+constexpr int sell_p() { return sizeof(FX) == 8 ? 2 : 4; }
 template <typename F, typename FX, typename I, int NV, int VK, typename V, class Epi>
 static void launch_sell(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s,
                         uint32_t chunk) {
     constexpr int H = 32 / (NV / VK);
     const DSell *S = sell_of<I, V>(A, H, s);
-    auto kern = k::k_spmv_sell<F, FX, I, NV, VK, SELL_P, Epi, V>;
+    auto kern = k::k_spmv_sell<F, FX, I, NV, VK, sell_p<FX>(), Epi, V>;
     const int res = resident_blocks(kern, 256, 0);
     const uint64_t chunks = (S->units + chunk - 1) / chunk;
     const uint32_t grid =

@@ -55,7 +55,7 @@ EXT_SYMBOLS = [
     "XAMG_b200_solver_hierarchy_export", "XAMG_b200_vector_device_ptr",
     "XAMG_b200_solver_level_csr", "XAMG_b200_kernel_launches", "XAMG_b200_stream",
     "XAMG_b200_set_device", "XAMG_b200_dot_noalloc", "XAMG_b200_wait_selftest",
-    "XAMG_b200_kernel_arch",
+    "XAMG_b200_kernel_arch", "XAMG_b200_grid_selftest",
     "XAMG_b200_solver_level_spmv", "XAMG_b200_read_system_size", "XAMG_b200_read_system",
     "XAMG_b200_write_system", "XAMG_b200_solver_hierarchy_save",
     "XAMG_b200_matrix_hierarchy_load", "XAMG_b200_gemm_bf16", "XAMG_b200_mlp_create",
@@ -177,6 +177,7 @@ def lib():
         "XAMG_b200_set_device": (C.c_int, [C.c_int]),
         "XAMG_b200_wait_selftest": (C.c_int, [C.c_double, C.POINTER(C.c_int)]),
         "XAMG_b200_kernel_arch": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "XAMG_b200_grid_selftest": (C.c_int, [C.c_double, C.POINTER(C.c_int)]),
         "XAMG_b200_solver_level_spmv": (C.c_int, [C.c_size_t, C.c_int, C.c_int, vp, vp, C.c_int,
                                                   C.c_int, vp]),
         "XAMG_b200_read_system_size": (C.c_int, [C.c_char_p, C.POINTER(C.c_uint32),
@@ -306,7 +307,7 @@ class Params:
                 "mg_interpolation_type", "mg_Pmax_elements", "mg_agg_num_levels",
                 "mg_agg_interpolation_type", "mg_agg_Pmax_elements", "mg_agg_P12max_elements",
                 "gpu_precond_f32", "gpu_coarse_f64", "gpu_index_compress", "gpu_hsgs_rows",
-                "gpu_graph", "gpu_seed"}
+                "gpu_graph", "gpu_seed", "gpu_persistent", "gpu_spmv_tune", "gpu_level_bf16"}
 
     def __init__(self, spec=None, overrides=None, set_default=True):
         h = sz()
