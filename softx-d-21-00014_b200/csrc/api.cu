@@ -48,7 +48,7 @@ struct MatObj {
     // device copies keyed by the narrowing switch and the tuning switch
     std::map<int, std::unique_ptr<DCsr>> dev;
     const DCsr *device(int narrow, int tune) {
-        auto &p = dev[narrow * 4 + tune];
+        auto &p = dev[narrow * 2 + (tune ? 1 : 0)];
         if (!p) {
             p.reset(new DCsr());
             upload_csr(h, *p, false, narrow, ctx().stream, tune);

@@ -125,22 +125,6 @@ struct DVec {
     uint64_t elems() const { return n * (uint64_t)nv; }
 };
 
-// Sliced (SELL) copy of a CSR block for the SpMVs without dot products,
-// built on the device on first use for one unit height H (the rows one warp
-// walks together): unit u holds rows [u*H, u*H + H) with its entries stored
-// entry-major, entry j of the unit's row q at off[u] + j*H + q, every row
-// padded to the unit's widest one (the pads are never read). A warp then
-// reads the j-th entries of its H rows as one contiguous load, with no
-// shared-memory staging and no block barrier. Packed: 2-byte columns and
-// 2-byte values share one 32-bit word (column in the low half).
-struct DSell {
-    int H = 0;
-    uint64_t units = 0, entries = 0;
-    bool packed = false;
-    DevBuf off;       // uint32_t [units + 1]
-    DevBuf col, val;  // entry-major arrays (packed: col holds both)
-};
-
 // A CSR block on the device with XAMG's narrowed column type.
 struct DCsr {
     uint64_t nrows = 0, ncols = 0, nnz = 0;
@@ -158,13 +142,8 @@ struct DCsr {
     // else 1 + 9 * (right-hand sides a thread: 0 default, 1 alternative) +
     // 3 * (staging: 0 one buffer, 1 two, 2 none) + (tile run: 0 one, 1 four,
     // 2 sixteen)
-    // else, from 19: the sliced kernel (k_spmv_sell) with chunk
-    // SELL_CHUNKS[code - 19] units a block
     bool tune_on = false;
-    bool force_sell = false;  // gpu_spmv_tune = 2: the sliced kernel, untimed
     mutable uint8_t tuned[2][2][6] = {};
-    // sliced copies built by the autotuner, per log2(unit height)
-    mutable std::shared_ptr<DSell> sell[6];
 
     template <typename F>
     k::CsrArgs<F> args() const {
@@ -184,7 +163,6 @@ struct DCsr {
 // shape by measurement (gpu_spmv_tune).
 // bf16 (with f32): store the values rounded to float and then to BF16
 // (round to nearest even), the arithmetic staying in float.
-// tune: 0 none, 1 measured launch shape, 2 always the sliced kernel.
 void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s, int tune = 0,
                 bool bf16 = false);
 void download_csr(const DCsr &d, uint32_t *row, void *col, void *val);

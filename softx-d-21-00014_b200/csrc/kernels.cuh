@@ -289,15 +289,26 @@ __device__ __forceinline__ F val_as(V v) {
         return (F)v;
 }
 
+// Column index in 32 bits (the launcher checks that every x offset c*NV + k
+// fits): the gather address is one 32-bit multiply-add and one widening add.
+template <typename I>
+__device__ __forceinline__ uint32_t col_at32(I c, uint32_t i) {
+    if constexpr (std::is_same<I, int16_t>::value)
+        return (uint32_t)((int32_t)i + (int32_t)c);
+    else
+        return (uint32_t)c;
+}
+
 template <typename F, typename FX, typename I, int NV, int VK, typename V = F>
 __device__ __forceinline__ void row_sum(F (&y)[VK], uint32_t len, uint64_t i, int k0, const I *cl,
                                         const V *vl, const FX *x) {
+    const uint32_t i32 = (uint32_t)i;
 #pragma unroll SPMV_UNROLL
     for (uint32_t j = 0; j < len; ++j) {
-        const uint64_t c = col_at<I>(cl[j], i);
+        const uint32_t c = col_at32<I>(cl[j], i32);
         const F av = val_as<F, V>(vl[j]);
         FX xv[VK];
-        ld_x<FX, VK>(x + c * NV + k0, xv);
+        ld_x<FX, VK>(x + (c * (uint32_t)NV + (uint32_t)k0), xv);
 #pragma unroll
         for (int v = 0; v < VK; ++v) y[v] = add(y[v], mul((F)xv[v], av));
     }
@@ -523,180 +534,6 @@ __global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
             for (uint32_t u = n_used; u < n_issued; ++u) mbar_wait(&mbar[u % nbuf], (u / nbuf) & 1u);
     }
     if constexpr (NRED > 0) canon_final<F, NV, NRED, CT / VK>(ra, B, epi);
-}
-
-// --- sliced SpMV (SELL copy of the matrix, SpMVs without dot products) ------
-// A warp walks one unit of H = 32 / G consecutive rows (G = NV / VK threads a
-// row): at step j it reads the j-th entries of its H rows as one contiguous
-// load (no staging, no block barrier; the next steps' entries are loaded
-// while this step's x gathers run), gathers x for them and accumulates each
-// row over its own entries in CSR order with separately rounded multiplies
-// and adds, as k_spmv does, so every result is the same bit for bit. A block takes chunks of `chunk`
-// consecutive units (its warps interleaved over the chunk, so that the warps
-// sharing an SM's L1 work on neighbouring rows); the grid is one wave.
-template <typename I, typename V>
-struct SellArgs {
-    const uint32_t *off;  // units + 1 entry offsets
-    const void *col;      // I[], or the packed words
-    const V *val;
-    const uint32_t *row;  // CSR row pointers: each row's length
-    uint64_t n;
-};
-
-// Streaming loads of the matrix entries: read once, kept out of L1 so that
-// L1 holds x.
-__device__ __forceinline__ uint32_t ld_na(const uint32_t *p) {
-    uint32_t r;
-    asm("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(r) : "l"(p));
-    return r;
-}
-__device__ __forceinline__ uint16_t ld_na(const uint16_t *p) {
-    uint16_t r;
-    asm("ld.global.nc.L1::no_allocate.b16 %0, [%1];" : "=h"(r) : "l"(p));
-    return r;
-}
-__device__ __forceinline__ int16_t ld_na(const int16_t *p) {
-    return (int16_t)ld_na((const uint16_t *)p);
-}
-__device__ __forceinline__ uint8_t ld_na(const uint8_t *p) {
-    uint32_t r;
-    asm("ld.global.nc.L1::no_allocate.u8 %0, [%1];" : "=r"(r) : "l"(p));
-    return (uint8_t)r;
-}
-__device__ __forceinline__ float ld_na(const float *p) {
-    float r;
-    asm("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(r) : "l"(p));
-    return r;
-}
-__device__ __forceinline__ double ld_na(const double *p) {
-    double r;
-    asm("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(r) : "l"(p));
-    return r;
-}
-__device__ __forceinline__ __nv_bfloat16 ld_na(const __nv_bfloat16 *p) {
-    return __ushort_as_bfloat16(ld_na((const uint16_t *)p));
-}
-
-// One unit's entries j .. j+P-1 of row q (those below len), loaded ahead of
-// their use.
-template <typename I, typename V, int H, int P, bool PACKED>
-__device__ __forceinline__ void sell_load(I (&cc)[P], V (&vv)[P], const uint32_t *pk, const I *col,
-                                          const V *val, uint32_t base, uint32_t j, uint32_t len,
-                                          int q) {
-#pragma unroll
-    for (int p = 0; p < P; ++p) {
-        if (j + p < len) {
-            const uint32_t e = base + (j + p) * H + q;
-            if constexpr (PACKED) {
-                const uint32_t w = ld_na(pk + e);
-                cc[p] = (I)(uint16_t)(w & 0xffffu);
-                if constexpr (std::is_same<V, __nv_bfloat16>::value)
-                    vv[p] = __ushort_as_bfloat16((unsigned short)(w >> 16));
-                else
-                    vv[p] = (V)(uint16_t)(w >> 16);
-            } else {
-                cc[p] = ld_na(col + e);
-                vv[p] = ld_na(val + e);
-            }
-        }
-    }
-}
-
-template <typename F, typename FX, typename I, int NV, int VK, int P, class Epi, typename V = F>
-__global__ void __launch_bounds__(256, 4)
-    k_spmv_sell(SellArgs<I, V> S, const FX *__restrict__ x, Epi epi, uint32_t chunk) {
-    constexpr int G = NV / VK;
-    constexpr int H = 32 / G;
-    constexpr bool PACKED = sizeof(I) == 2 && sizeof(V) == 2;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int q = lane / G, k0 = (lane % G) * VK;
-    const uint64_t n = S.n;
-    const uint64_t units = (n + H - 1) / H;
-    const uint32_t *__restrict__ off = S.off;
-    const uint32_t *__restrict__ row = S.row;
-    const uint32_t *__restrict__ pk = (const uint32_t *)S.col;
-    const I *__restrict__ col = (const I *)S.col;
-    const V *__restrict__ val = S.val;
-    F dummy[1];
-    for (uint64_t c = blockIdx.x; c * chunk < units; c += gridDim.x) {
-        const uint64_t u1 = (c + 1) * chunk < units ? (c + 1) * chunk : units;
-        for (uint64_t u = c * chunk + warp; u < u1; u += nw) {
-            const uint64_t i = u * H + q;
-            const bool live = i < n;
-            const uint32_t len = live ? __ldg(&row[i + 1]) - __ldg(&row[i]) : 0u;
-            const uint32_t base = __ldg(&off[u]);
-            const uint32_t width = (__ldg(&off[u + 1]) - base) / H;
-            F y[VK];
-#pragma unroll
-            for (int v = 0; v < VK; ++v) y[v] = live ? epi.init(i, k0 + v) : F(0);
-            // the next P entries are in flight while this step's x gathers
-            // and sums run
-            I cc[P], cn[P];
-            V vv[P], vn[P];
-            sell_load<I, V, H, P, PACKED>(cc, vv, pk, col, val, base, 0, len, q);
-            for (uint32_t j = 0; j < width; j += P) {
-                FX xv[P][VK];
-#pragma unroll
-                for (int p = 0; p < P; ++p)
-                    if (j + p < len) ld_x<FX, VK>(x + col_at<I>(cc[p], i) * NV + k0, xv[p]);
-                sell_load<I, V, H, P, PACKED>(cn, vn, pk, col, val, base, j + P, len, q);
-#pragma unroll
-                for (int p = 0; p < P; ++p)
-                    if (j + p < len) {
-                        const F a = val_as<F, V>(vv[p]);
-#pragma unroll
-                        for (int v = 0; v < VK; ++v) y[v] = add(y[v], mul((F)xv[p][v], a));
-                    }
-#pragma unroll
-                for (int p = 0; p < P; ++p) {
-                    cc[p] = cn[p];
-                    vv[p] = vn[p];
-                }
-            }
-            if (live) {
-#pragma unroll
-                for (int v = 0; v < VK; ++v) epi.store(i, k0 + v, y[v], dummy);
-            }
-        }
-    }
-}
-
-// Width of every unit of H rows (its longest row).
-static __global__ void k_sell_width(const uint32_t *__restrict__ row, uint64_t n, int H,
-                                    uint32_t *__restrict__ w) {
-    const uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint64_t units = (n + H - 1) / H;
-    if (u >= units) return;
-    uint32_t m = 0;
-    for (uint64_t i = u * H; i < (u + 1) * H && i < n; ++i) {
-        const uint32_t l = row[i + 1] - row[i];
-        m = l > m ? l : m;
-    }
-    w[u] = m;
-}
-
-// Scatter of the CSR entries into the unit-major layout (one thread a row);
-// packed: the 2-byte column in the low and the 2-byte value in the high half.
-template <typename I, typename V, bool PACKED>
-__global__ void k_sell_fill(const uint32_t *__restrict__ row, const I *__restrict__ col,
-                            const V *__restrict__ val, uint64_t n, int H,
-                            const uint32_t *__restrict__ off, void *scol, V *sval) {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint64_t u = i / H, q = i % H;
-    const uint32_t base = off[u];
-    for (uint32_t j = row[i]; j < row[i + 1]; ++j) {
-        const uint64_t e = base + (uint64_t)(j - row[i]) * H + q;
-        if constexpr (PACKED) {
-            uint16_t cv, vvb;
-            memcpy(&cv, &col[j], 2);
-            memcpy(&vvb, &val[j], 2);
-            ((uint32_t *)scol)[e] = (uint32_t)cv | ((uint32_t)vvb << 16);
-        } else {
-            ((I *)scol)[e] = col[j];
-            sval[e] = val[j];
-        }
-    }
 }
 
 // Bounded-wait check: one block waits on an mbarrier that nothing arrives
@@ -1493,7 +1330,9 @@ __device__ __forceinline__ void canon_final_local(const double *part, uint32_t B
 
 struct PersistArgs {
     double *x, *r0, *r, *p, *v, *s, *t, *pa, *sa, *tmp;
-    const double *d;   // Jacobi inverse diagonal; null: no preconditioner (pa = p, sa = s)
+    const double *d;   // Jacobi inverse diagonal; null: no Jacobi preconditioner
+    int ident;         // with d null: 1 the Identity preconditioner (pa, sa copies of p, s),
+                       // 0 none (pa = p, sa = s)
     double relax;
     int sweeps;        // Jacobi sweeps (max_iters of the preconditioner list)
     double *sc;        // the solver's scalar block: read at the start, written at the end
@@ -1562,10 +1401,16 @@ __global__ void __launch_bounds__(CT, 1) k_pbicgstab_persist(CsrArgs<double> A, 
         return true;
     };
     // out = M^-1 in: Jacobi sweeps from zero (jacobi.inl:113-119,
-    // blas_merged_jacobi.inl), the last landing in out; without a
-    // preconditioner pa/sa are p/s themselves
+    // blas_merged_jacobi.inl), the last landing in out; the Identity copies;
+    // without a preconditioner pa/sa are p/s themselves
     auto precond = [&](double *out, const double *in) {
-        if (!P.d) return true;
+        if (!P.d) {
+            if (P.ident) {  // Identity::solve: x = b (ops::convert)
+                const OpConvert<double, double> cp{out, in};
+                each([&](uint64_t, uint64_t e) { cp(e); });
+            }
+            return true;
+        }
         const int m = P.sweeps < 1 ? 1 : P.sweeps;
         auto tgt = [&](int j) { return ((m - j) % 2 == 0) ? out : P.tmp; };
         double *cur = tgt(1);

@@ -228,7 +228,6 @@ template void axpy_k<float>(float *, const float *, const double *, uint64_t, in
 void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s, int tune,
                 bool bf16) {
     d.tune_on = tune != 0;
-    d.force_sell = tune == 2;
     d.bf16 = f32 && bf16;
     d.nrows = h.nrows;
     d.ncols = h.ncols;

@@ -977,14 +977,15 @@ bool Krylov::started() {
 }
 
 // gpu_persistent (default 1): the preconditioned forms (PBiCGStab,
-// MergedPBiCGStab) with no preconditioner or a Jacobi preconditioner without
-// its own convergence test run every iteration in one cooperative launch
+// MergedPBiCGStab) with the Identity (no preconditioner list) or a Jacobi
+// preconditioner without its own convergence test run every iteration in
+// one cooperative launch
 // when the matrix's canonical blocks fit the GPU at once (small and
 // mid-sized systems; the 32^3 Poisson system has 128); printing residuals
 // (convergence_info) keeps the host loop.
 bool Krylov::persistent_ok() const {
     if (!cfg.gpu_persistent || !precond_form || cfg.convergence_info || f32) return false;
-    if (M) {
+    if (M && !dynamic_cast<const Identity<double> *>(M.get())) {
         auto *j = dynamic_cast<const Jacobi<double> *>(M.get());
         if (!j || j->cfg.convergence_check || j->f32) return false;
     }
@@ -1010,6 +1011,7 @@ void Krylov::run_persistent(DVec &x) {
     P.sa = M ? buf[7].p<double>() : P.s;
     P.tmp = jac ? jac->buf[1].p<double>() : nullptr;
     P.d = jac ? jac->d.as<double>() : nullptr;
+    P.ident = (M && !jac) ? 1 : 0;
     P.relax = jac ? (double)jac->cfg.relax : 0.0;
     P.sweeps = jac ? std::max(1, jac->cfg.max_iters) : 0;
     P.sc = sc.as<double>();

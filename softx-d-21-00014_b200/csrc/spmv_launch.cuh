@@ -103,6 +103,9 @@ static void launch_vk(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s
                       uint32_t nbuf_force = 0, uint32_t run = 1) {
     constexpr uint32_t LIMIT1 = (96u * 1024u - 64u) / (uint32_t)(sizeof(V) + sizeof(I));
     constexpr int NT = k::CT / VK;
+    // the kernel forms x offsets c*NV + k and row indices in 32 bits
+    XG_REQUIRE(std::max(A.ncols, A.nrows) * (uint64_t)NV < (1ull << 32), XAMG_ERR_UNSUPPORTED,
+               "SpMV: x of 2^32 or more values");
     auto kern = k::k_spmv<F, FX, I, NV, VK, NRED, Epi, V>;
     static bool big_smem = false;  // one flag per instantiation
     if (!big_smem) {
@@ -132,79 +135,6 @@ static void launch_vk(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s
                                 : (uint32_t)std::min<uint64_t>((ntiles + run - 1) / run, wave);
     const uint32_t P = (uint32_t)std::min<uint64_t>(B, wave);
     kern<<<P, NT, smem, s>>>(A.args<F>(), x, epi, ctx().red(), cap, nbuf, B, run);
-    XG_CUDA(cudaGetLastError());
-    ++g_kernel_launches;
-}
-
-// Sliced copy of A for units of H rows, built on the device on first use
-// (outside any graph capture: the autotuner builds it before a tuned code
-// can name it). Padded entries stay unwritten: no kernel reads them.
-template <typename I, typename V>
-static const DSell *sell_of(const DCsr &A, int H, cudaStream_t s) {
-    int l = 0;
-    while ((1 << l) < H) ++l;
-    if (A.sell[l]) return A.sell[l].get();
-    auto d = std::make_shared<DSell>();
-    d->H = H;
-    d->units = (A.nrows + H - 1) / H;
-    d->packed = sizeof(I) == 2 && sizeof(V) == 2;
-    DevBuf w(d->units * sizeof(uint32_t));
-    k::k_sell_width<<<(unsigned)((d->units + 255) / 256), 256, 0, s>>>(A.row.as<uint32_t>(),
-                                                                       A.nrows, H,
-                                                                       w.as<uint32_t>());
-    XG_CUDA(cudaGetLastError());
-    std::vector<uint32_t> wh(d->units);
-    XG_CUDA(cudaMemcpyAsync(wh.data(), w.p, w.bytes, cudaMemcpyDeviceToHost, s));
-    XG_CUDA(cudaStreamSynchronize(s));
-    std::vector<uint32_t> off(d->units + 1, 0);
-    uint64_t total = 0;
-    for (uint64_t u = 0; u < d->units; ++u) {
-        off[u] = (uint32_t)total;
-        total += (uint64_t)wh[u] * (uint64_t)H;
-        XG_REQUIRE(total < (1ull << 32), XAMG_ERR_UNSUPPORTED,
-                   "sliced SpMV copy needs more than 2^32 entries");
-    }
-    off[d->units] = (uint32_t)total;
-    d->entries = total;
-    upload(d->off, off, s);
-    d->col.alloc(std::max<uint64_t>(1, total) * (d->packed ? 4 : sizeof(I)));
-    if (!d->packed) d->val.alloc(std::max<uint64_t>(1, total) * sizeof(V));
-    const unsigned g = (unsigned)((A.nrows + 255) / 256);
-    if constexpr (sizeof(I) == 2 && sizeof(V) == 2)
-        k::k_sell_fill<I, V, true><<<g, 256, 0, s>>>(A.row.as<uint32_t>(), (const I *)A.col.p,
-                                                     (const V *)A.val.p, A.nrows, H,
-                                                     d->off.as<uint32_t>(), d->col.p, nullptr);
-    else
-        k::k_sell_fill<I, V, false><<<g, 256, 0, s>>>(A.row.as<uint32_t>(), (const I *)A.col.p,
-                                                      (const V *)A.val.p, A.nrows, H,
-                                                      d->off.as<uint32_t>(), d->col.p,
-                                                      d->val.as<V>());
-    XG_CUDA(cudaGetLastError());
-    XG_CUDA(cudaStreamSynchronize(s));
-    A.sell[l] = d;
-    return d.get();
-}
-
-// The sliced kernel: 256-thread blocks, a wave of them, chunks of `chunk`
-// units a block.
-constexpr uint32_t SELL_CHUNKS[3] = {8, 64, 512};
-// entries whose loads a warp issues together (fewer for FP64, within 64
-// registers a thread)
-template <typename FX>
-constexpr int sell_p() { return sizeof(FX) == 8 ? 2 : 4; }
-template <typename F, typename FX, typename I, int NV, int VK, typename V, class Epi>
-static void launch_sell(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s,
-                        uint32_t chunk) {
-    constexpr int H = 32 / (NV / VK);
-    const DSell *S = sell_of<I, V>(A, H, s);
-    auto kern = k::k_spmv_sell<F, FX, I, NV, VK, sell_p<FX>(), Epi, V>;
-    const int res = resident_blocks(kern, 256, 0);
-    const uint64_t chunks = (S->units + chunk - 1) / chunk;
-    const uint32_t grid =
-        (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(chunks, (uint64_t)res * ctx().sms));
-    kern<<<grid, 256, 0, s>>>(k::SellArgs<I, V>{S->off.as<uint32_t>(), S->col.p, S->val.as<V>(),
-                                                A.row.as<uint32_t>(), A.nrows},
-                              x, epi, chunk);
     XG_CUDA(cudaGetLastError());
     ++g_kernel_launches;
 }
@@ -275,25 +205,6 @@ static uint8_t autotune(const DCsr &A, const FX *x, cudaStream_t s) {
                     code = (uint8_t)(1 + alt * 9 + (nb - 1) * 3 + ri);
                 }
             }
-    // the sliced kernel, in chunks of 8, 64 or 512 units a block
-    for (int ci = 0; ci < 3; ++ci) {
-        auto go = [&] { launch_sell<F, FX, I, NV, VD, V>(A, x, e, s, SELL_CHUNKS[ci]); };
-        float ms = 1e30f;
-        go();
-        for (int round = 0; round < 2; ++round) {
-            XG_CUDA(cudaEventRecord(e0, s));
-            for (int r = 0; r < 3; ++r) go();
-            XG_CUDA(cudaEventRecord(e1, s));
-            XG_CUDA(cudaEventSynchronize(e1));
-            float t = 0;
-            XG_CUDA(cudaEventElapsedTime(&t, e0, e1));
-            ms = std::min(ms, t);
-        }
-        if (ms < best) {
-            best = ms;
-            code = (uint8_t)(19 + ci);
-        }
-    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     XG_CUDA(cudaStreamSynchronize(s));
@@ -317,11 +228,7 @@ static void launch_v(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s)
             int l = 0;
             while ((1 << l) < NV) ++l;
             uint8_t &t = A.tuned[sizeof(F) == 4][sizeof(FX) == 4][l];
-            if (!t) t = A.force_sell ? (uint8_t)20 : autotune<F, FX, I, NV, V>(A, x, s);
-            if (t >= 19) {
-                launch_sell<F, FX, I, NV, VK, V>(A, x, epi, s, SELL_CHUNKS[t - 19]);
-                return;
-            }
+            if (!t) t = autotune<F, FX, I, NV, V>(A, x, s);
             if (t) {
                 const Tuned c = tuned_shape(t);
                 if (c.alt)

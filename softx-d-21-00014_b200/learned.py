@@ -144,19 +144,36 @@ def fp64_transfer_params(tol):
     return p
 
 
+def vcycle_params():
+    """One V(1,1) cycle of the same hierarchy as a stationary step from the
+    given x: x + M^-1 (b - A x) with the multigrid preconditioner M (FP64)."""
+    sm = {"method": "Chebyshev", "polynomial_order": 2}
+    return {"solver": {"method": "MultiGrid", "max_iters": 1, "convergence_check": 0,
+                       "mg_agg_num_levels": 0, "mg_strength_threshold": 0.25,
+                       "mg_coarsening_type": 8, "mg_interpolation_type": 6,
+                       "mg_coarse_matrix_size": 500, "mg_reduced_precision": 0},
+            "pre_smoother": sm, "post_smoother": dict(sm),
+            "coarse_grid_solver": {"method": "Direct"}}
+
+
 def run(n_edge=96, n_train=4096, n_eval=1024, nv=32, steps=400, level=3, hidden=1024,
-        sigma=1.0, seed=0, train_tol=1e-10, tol=1e-8, lr=1e-3, batch=512, log=print):
+        sigma=1.0, seed=0, train_tol=1e-10, tol=1e-8, lr=1e-3, batch=512, log=print,
+        smoothing="vcycle"):
     """Trains the guess on n_train solved right-hand sides and compares it with
-    the zero guess on n_eval held-out ones (all in blocks of nv). Returns a
-    dict of iterations, ms per right-hand side and initial residuals."""
+    the zero guess on n_eval held-out ones (all in blocks of nv). smoothing:
+    what is applied to the prolongated guess before it is tested: "vcycle"
+    (one multigrid V-cycle step x0 + M^-1 (b - A x0), which removes the
+    high-frequency error the coarse coefficients leave) or "jacobi" (two
+    damped Jacobi sweeps). Returns a dict of iterations, ms per right-hand
+    side and initial residuals."""
     st = torch.cuda.ExternalStream(X.stream())
     with torch.cuda.stream(st):
         return _run(n_edge, n_train, n_eval, nv, steps, level, hidden, sigma, seed, train_tol,
-                    tol, lr, batch, log, st)
+                    tol, lr, batch, log, st, smoothing)
 
 
 def _run(n_edge, n_train, n_eval, nv, steps, level, hidden, sigma, seed, train_tol, tol, lr,
-         batch, log, st):
+         batch, log, st, smoothing):
     t_setup = time.time()
     row, col, val = X.generate_diffusion(7, n_edge, n_edge, n_edge, sigma, 1.0, seed)
     n = len(row) - 1
@@ -170,12 +187,16 @@ def _run(n_edge, n_train, n_eval, nv, steps, level, hidden, sigma, seed, train_t
     x1.set(0.0)
     b1.set(1.0)
     S64 = X.Solver(M, X.Params(fp64_transfer_params(tol)), x1, b1)
-    # two damped Jacobi sweeps on the prolongated guess (damps the
-    # high-frequency part of its residual that the coarse coefficients leave)
+    # the prolongated guess is smoothed before its residual is tested: the
+    # coarse coefficients leave high-frequency error that the multigrid
+    # cycle (or, more weakly, two damped Jacobi sweeps) removes
     xs, bs = X.Vector(n, nv), X.Vector(n, nv)
-    S_jac = X.Solver(M, X.Params({"solver": {"method": "Jacobi", "max_iters": 2,
-                                             "convergence_check": 0, "relax_factor": 0.8}}),
-                     xs, bs)
+    if smoothing == "jacobi":
+        S_smooth = X.Solver(M, X.Params({"solver": {"method": "Jacobi", "max_iters": 2,
+                                                    "convergence_check": 0,
+                                                    "relax_factor": 0.8}}), xs, bs)
+    else:
+        S_smooth = X.Solver(M, X.Params(vcycle_params()), xs, bs)
     nl = S64.nlevels()
     level = min(level, nl - 1)
     LG = LearnedGuess(S64, level, hidden, seed)
@@ -197,7 +218,7 @@ def _run(n_edge, n_train, n_eval, nv, steps, level, hidden, sigma, seed, train_t
     def smooth(x0):
         upload(xs, x0.contiguous())
         upload(bs, cur_b["b"])
-        S_jac.solve()
+        S_smooth.solve()
         return download(xs)
 
     # training pairs from the solver itself
@@ -257,6 +278,6 @@ def _run(n_edge, n_train, n_eval, nv, steps, level, hidden, sigma, seed, train_t
                learned_iters=float(np.mean(res["learned_iters"])),
                zero_ms_per_rhs=res["zero_ms"] / nrhs, learned_ms_per_rhs=res["learned_ms"] / nrhs,
                initial_residual_ratio=float(np.median(res["r0_ratio"])),
-               guesses_kept=res["kept"] / nrhs)
+               guesses_kept=res["kept"] / nrhs, smoothing=smoothing)
     log(out)
     return out
