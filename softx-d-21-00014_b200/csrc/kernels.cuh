@@ -838,19 +838,21 @@ struct EGroup2 {
 // beta = (scal1/rho)*(alpha/omega); rho = scal1; nscal = -(omega*beta);
 // and, for the unpreconditioned form, alpha_c/omega_c from the current iconv
 // (merged_bicgstab.inl:192-199).
-template <int NV, bool XUPD>
+// PT: the type the preconditioned vectors pa, sa are stored in (float when
+// an FP32 preconditioner leaves its result in float; widened exactly).
+template <int NV, bool XUPD, typename PT = double>
 struct EGroup4 {
     const double *s, *t, *r0;
     double *r;
     double *x;
-    const double *pa, *sa;
+    const PT *pa, *sa;
     double *sc;
     template <int NR>
     __device__ void elem(uint64_t i, int k, double (&acc)[NR]) const {
         const uint64_t e = i * NV + k;
         if constexpr (XUPD) {
             const double ac = sc[SC_ALPHA_C * SC_STRIDE + k], oc = sc[SC_OMEGA_C * SC_STRIDE + k];
-            x[e] = add(add(mul(ac, pa[e]), mul(oc, sa[e])), mul(1.0, x[e]));
+            x[e] = add(add(mul(ac, (double)pa[e]), mul(oc, (double)sa[e])), mul(1.0, x[e]));
         }
         const double om = sc[SC_OMEGA * SC_STRIDE + k];
         const double rv = sub(s[e], mul(om, t[e]));
@@ -899,16 +901,19 @@ struct OpSUpdate {
 };
 
 // x = alpha_c*pa + omega_c*sa + 1*x  (merged_pbicgstab.inl:193, blas_ext.inl:173-177)
-struct OpXUpdate {
+template <typename PT = double>
+struct OpXUpdateT {
     double *x;
-    const double *pa, *sa, *sc;
+    const PT *pa, *sa;
+    const double *sc;
     int nv;
     __device__ void operator()(uint64_t e) const {
         const int k = (int)(e % nv);
         const double ac = sc[SC_ALPHA_C * SC_STRIDE + k], oc = sc[SC_OMEGA_C * SC_STRIDE + k];
-        x[e] = add(add(mul(ac, pa[e]), mul(oc, sa[e])), mul(1.0, x[e]));
+        x[e] = add(add(mul(ac, (double)pa[e]), mul(oc, (double)sa[e])), mul(1.0, x[e]));
     }
 };
+using OpXUpdate = OpXUpdateT<double>;
 
 // PCG (pcg.inl:103-150). Ap = A p with scal2 = (p, Ap); finaliser:
 // alpha = scal1 / scal2, alpha_conv = iconv * alpha, then alpha = -1 * alpha
@@ -1342,6 +1347,20 @@ struct PersistArgs {
     RedArgs ra;        // partial sums: two halves used in turn
     GridSync gs;
 };
+
+// A BiCGStab solve recorded as one graph (csrc/loop.cu): the convergence
+// test's settings and the conditional handles it sets: loop (iterate again),
+// rest (the rest of a non-converged iteration), last (the final x update).
+struct LoopCtl {
+    int nv, max_iters, check;
+    float abs_tol, rel_tol;
+    cudaGraphConditionalHandle loop, rest, last;
+};
+// The statistics the loop leaves in device memory (doubles): abs_res,
+// rel_res and conv (0/1) per right-hand side, the iterations, and whether
+// the last test passed.
+constexpr int LOOP_ABS = 0, LOOP_REL = 32, LOOP_CONV = 64, LOOP_ITERS = 96, LOOP_DONE = 97,
+              LOOP_COUNT = 98;
 
 // merged_pbicgstab.inl:44-225 after its start (r0, rho0, p = r = r0 and the
 // first test, done by Krylov::begin/started): every iteration, its

@@ -22,6 +22,13 @@ void pbicgstab_persist(const DCsr &A, const k::PersistArgs &P, int nv, cudaStrea
 // limit_ns and raise *flag.
 void grid_selftest(unsigned *count_gen, unsigned *flag, uint64_t limit_ns, cudaStream_t s);
 
+// The convergence tests of a BiCGStab solve recorded as one graph
+// (csrc/loop.cu): after r0 = b - A x (loop_start) and after each iteration's
+// residual (loop_check); they set the graph's conditional handles in c and
+// keep the statistics in out (k::LOOP_* layout).
+void loop_start(double *sc, double *out, const k::LoopCtl &c, cudaStream_t s);
+void loop_check(double *sc, double *out, const k::LoopCtl &c, cudaStream_t s);
+
 // Resolves the fixed scratch array of XAMG_b200_dot_noalloc and loads its
 // kernels on the current device (csrc/noalloc.cu); returns an XAMG status.
 int noalloc_prepare_current_device();
@@ -46,6 +53,10 @@ void group1_zero(uint64_t n, const double *b, double *r0, double *p, double *r, 
 
 // v = A pa; scal1 = (v, r0); alpha = rho/scal1
 void spmv_dot_alpha(const DCsr &A, const double *pa, double *v, const double *r0, double *sc,
+                    int nv, cudaStream_t s);
+// ... with pa stored in float (an FP32 preconditioner's result, widened
+// exactly as it is read: the same sums)
+void spmv_dot_alpha(const DCsr &A, const float *pa, double *v, const double *r0, double *sc,
                     int nv, cudaStream_t s);
 
 // t = A sa; phi, psi, theta; omega; res; alpha_c; omega_c
@@ -78,6 +89,8 @@ void gemm_bf16(uint64_t M, uint64_t N, uint64_t K, const void *A, const void *B,
 }  // namespace mm
 
 void spmv_dot3(const DCsr &A, const double *sa, double *t, const double *s_, double *sc, int nv,
+               cudaStream_t s);
+void spmv_dot3(const DCsr &A, const float *sa, double *t, const double *s_, double *sc, int nv,
                cudaStream_t s);
 
 // One Jacobi sweep xout = xin + relax*d*(b - A xin)
@@ -118,10 +131,14 @@ void group2(uint64_t n, const double *t, const double *s_, double *out96, int nv
 void group4(uint64_t n, const double *s_, const double *t, const double *r0, double *r,
             double *x, const double *pa, const double *sa, bool with_x, double *sc, int nv,
             cudaStream_t s);
+void group4(uint64_t n, const double *s_, const double *t, const double *r0, double *r,
+            double *x, const float *pa, const float *sa, double *sc, int nv, cudaStream_t s);
 void s_update(uint64_t n, double *s_, const double *r, const double *v, const double *sc, int nv,
               cudaStream_t s);
 void x_update(uint64_t n, double *x, const double *pa, const double *sa, const double *sc,
               int nv, cudaStream_t s);
+void x_update(uint64_t n, double *x, const float *pa, const float *sa, const double *sc, int nv,
+              cudaStream_t s);
 void p_update(uint64_t n, double *p, const double *r, const double *v, const double *sc, int nv,
               cudaStream_t s);
 void group5(uint64_t n, double *x, double *p, const double *s_, const double *r, const double *v,

@@ -49,6 +49,18 @@ void spmv_dot_alpha(const DCsr &A, const double *pa, double *v, const double *r0
     });
 }
 
+void spmv_dot_alpha(const DCsr &A, const float *pa, double *v, const double *r0, double *sc,
+                    int nv, cudaStream_t s) {
+    XG_DISPATCH(A, nv, {
+        launch<double, float, I, NV, 1>(A, pa, k::EDotAlpha<NV>{v, r0, sc}, s);
+    });
+}
+
+void spmv_dot3(const DCsr &A, const float *sa, double *t, const double *s_, double *sc, int nv,
+               cudaStream_t s) {
+    XG_DISPATCH(A, nv, { launch<double, float, I, NV, 3>(A, sa, k::EDot3<NV>{t, s_, sc}, s); });
+}
+
 void pcg_ap(const DCsr &A, const double *p, double *Ap, double *sc, int nv, cudaStream_t s) {
     XG_DISPATCH(A, nv, { launch<double, double, I, NV, 1>(A, p, k::EPcgAp<NV>{Ap, p, sc}, s); });
 }
@@ -90,6 +102,14 @@ void group2(uint64_t n, const double *t, const double *s_, double *out96, int nv
     dispatch_nv(nv, [&](auto nvc) {
         constexpr int NV = decltype(nvc)::value;
         launch_rows<double, NV, 3>(n, k::EGroup2<NV>{t, s_, out96}, s);
+    });
+}
+
+void group4(uint64_t n, const double *s_, const double *t, const double *r0, double *r,
+            double *x, const float *pa, const float *sa, double *sc, int nv, cudaStream_t s) {
+    dispatch_nv(nv, [&](auto nvc) {
+        constexpr int NV = decltype(nvc)::value;
+        launch_rows<double, NV, 1>(n, k::EGroup4<NV, true, float>{s_, t, r0, r, x, pa, sa, sc}, s);
     });
 }
 

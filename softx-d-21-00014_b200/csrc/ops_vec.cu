@@ -138,6 +138,10 @@ void x_update(uint64_t n, double *x, const double *pa, const double *sa, const d
               int nv, cudaStream_t s) {
     flat(n * nv, k::OpXUpdate{x, pa, sa, sc, nv}, s);
 }
+void x_update(uint64_t n, double *x, const float *pa, const float *sa, const double *sc, int nv,
+              cudaStream_t s) {
+    flat(n * nv, k::OpXUpdateT<float>{x, pa, sa, sc, nv}, s);
+}
 void p_update(uint64_t n, double *p, const double *r, const double *v, const double *sc, int nv,
               cudaStream_t s) {
     flat(n * nv, k::OpPUpdate{p, r, v, sc, nv}, s);

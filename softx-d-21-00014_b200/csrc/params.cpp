@@ -80,6 +80,7 @@ static const std::map<std::string, KeyInfo> &dictionary() {
         {"gpu_level_bf16", {'I', "", "0", "50", ""}},
         {"gpu_seed", {'I', "", "", "", ""}},
         {"gpu_persistent", {'I', "", "0", "1", ""}},
+        {"gpu_solve_graph", {'I', "", "0", "1", ""}},
     };
     return d;
 }
@@ -359,6 +360,7 @@ SolverCfg resolve_cfg(const PList &l, const std::string &role) {
     c.gpu_level_bf16 = l.get_i("gpu_level_bf16", 0);
     c.gpu_seed = l.get_i("gpu_seed", 0);
     c.gpu_persistent = l.get_i("gpu_persistent", 1);
+    c.gpu_solve_graph = l.get_i("gpu_solve_graph", 1);
     return c;
 }
 

@@ -86,6 +86,7 @@ struct SolverCfg {
     int gpu_level_bf16 = 0;     // finest FP32 cycle levels whose matrix values are BF16
     int gpu_seed = 0;           // seed of the host setup's random choices
     int gpu_persistent = 1;     // eligible BiCGStab solves in one cooperative launch
+    int gpu_solve_graph = 1;    // whole BiCGStab solves as one graph with a device-side loop
 };
 
 SolverCfg resolve_cfg(const PList &l, const std::string &role);

@@ -651,6 +651,22 @@ void MultiGrid::cycle(int level, DVec &x, DVec &b, int cyc, const std::vector<do
     post[level]->solve(x, b, iconv);
 }
 
+// The gpu_precond_f32 = 1 preconditioner with its result left in float in
+// x32 (a caller's buffer): the same cycles as solve(); a caller that reads
+// x32 widened exactly sees the values solve() would write into x.
+void MultiGrid::solve_to32(DVec &x32o, DVec &b, const std::vector<double> &conv) {
+    reset_stats();
+    std::vector<double> iconv = conv;
+    b32.zero = b.zero;
+    if (!b.zero) ops::convert<float, double>(b32.p<float>(), b.p<double>(), b.elems(), S());
+    b32.init = true;
+    x32o.init = true;
+    do {
+        ++st.iters;
+        cycle(0, x32o, b32, cfg.mg_cycle, iconv);
+    } while (st.iters < cfg.max_iters);
+}
+
 // mg.inl:262-334
 void MultiGrid::solve(DVec &x, DVec &b, const std::vector<double> &conv) {
     reset_stats();
@@ -713,7 +729,24 @@ bool Krylov::check(const double *res, const double *res0, std::vector<double> &i
 void Krylov::run_M(DVec &out, DVec &in) {
     static const std::vector<double> ones(32, 1.0);
     std::vector<double> o(ones.begin(), ones.begin() + NV);
-    M->solve(out, in, o);
+    if (f32io && out.f32)
+        static_cast<MultiGrid *>(M.get())->solve_to32(out, in, o);
+    else
+        M->solve(out, in, o);
+}
+
+// An FP32 multigrid preconditioner (gpu_precond_f32 = 1) whose cycle never
+// reads its output's old contents (V- and W-cycles; the F-cycle adds to
+// them) leaves its results in float: the Krylov kernels then read pa32/sa32
+// widened to double, exactly the values converting them back to FP64 would
+// write, without that conversion and with half the bytes in the SpMV's x
+// gathers. The merged BiCGStab forms only (PCG and RBiCGStab keep FP64).
+void Krylov::enable_f32io() {
+    auto *g = dynamic_cast<MultiGrid *>(M.get());
+    if (!g || !g->full32 || pcg || rbicgstab || !precond_form) return;
+    f32io_ready = true;
+    pa32.alloc(n, NV, true);
+    sa32.alloc(n, NV, true);
 }
 
 Krylov::~Krylov() {
@@ -947,6 +980,8 @@ void Krylov::solve(DVec &x, DVec &b, const std::vector<double> &conv) {
 // merged_bicgstab.inl:44-208 / merged_pbicgstab.inl:44-225
 void Krylov::begin(DVec &x, DVec &b, const std::vector<double> &conv) {
     reset_stats();
+    // the cycle type may have been renewed since the solver was built
+    f32io = f32io_ready && static_cast<MultiGrid *>(M.get())->cfg.mg_cycle != 1;
     cudaStream_t s = S();
     run_.x = &x;
     run_.b = &b;
@@ -1155,6 +1190,18 @@ void Krylov::step_body() {
          &p_ = buf[6], &s2 = buf[7];
     run_.pa = &p;
     run_.sa = &s_;
+    if (f32io) {
+        apply_M(pa32, p);
+        ops::spmv_dot_alpha(*A, pa32.p<float>(), v.p<double>(), r0.p<double>(), SC, NV, s);
+        v.zero = false;
+        ops::s_update(n, s_.p<double>(), r.p<double>(), v.p<double>(), SC, NV, s);
+        s_.zero = false;
+        apply_M(sa32, s_);
+        ops::spmv_dot3(*A, sa32.p<float>(), t.p<double>(), s_.p<double>(), SC, NV, s);
+        t.zero = false;
+        post_scalars(SC + k::SC_RES * k::SC_STRIDE, NV);
+        return;
+    }
     if (M) {
         apply_M(p_, p);
         run_.pa = &p_;
@@ -1186,7 +1233,9 @@ bool Krylov::stepped() {
         run_.tail = true;  // launched by the next step() or by finish()
         return false;
     }
-    if (precond_form)
+    if (f32io)
+        ops::x_update(n, x.p<double>(), pa32.p<float>(), sa32.p<float>(), SC, NV, s);
+    else if (precond_form)
         ops::x_update(n, x.p<double>(), run_.pa->p<double>(), run_.sa->p<double>(), SC, NV, s);
     else
         ops::x_update(n, x.p<double>(), p.p<double>(), s_.p<double>(), SC, NV, s);
@@ -1206,7 +1255,11 @@ void Krylov::step_tail() {
     double *SC = sc.as<double>();
     DVec &r0 = buf[0], &r = buf[1], &p = buf[2], &v = buf[3], &s_ = buf[4], &t = buf[5];
     DVec &x = *run_.x;
-    if (precond_form) {
+    if (f32io) {
+        ops::group4(n, s_.p<double>(), t.p<double>(), r0.p<double>(), r.p<double>(),
+                    x.p<double>(), pa32.p<float>(), sa32.p<float>(), SC, NV, s);
+        ops::p_update(n, p.p<double>(), r.p<double>(), v.p<double>(), SC, NV, s);
+    } else if (precond_form) {
         // x update fused with r = s - omega t; rho = (r, r0); beta
         ops::group4(n, s_.p<double>(), t.p<double>(), r0.p<double>(), r.p<double>(),
                     x.p<double>(), run_.pa->p<double>(), run_.sa->p<double>(), true, SC, NV, s);
@@ -1280,6 +1333,7 @@ void SolverHierarchy::build(const Params &P, const HCsr &hA_, const DCsr *A_, in
             ic.method = "Identity";
             kr->M = make_smoother(ic, "preconditioner", *A, hA, false, nv, 0, 0);
         }
+        kr->enable_f32io();
         root.reset(kr);
         return;
     }

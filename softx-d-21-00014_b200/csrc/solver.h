@@ -74,6 +74,9 @@ class MultiGrid : public SolverBase {
     void build(const HCsr &A0, const DCsr *A0dev, const Params &P, const std::string &role,
                int nv, HierCache *cache);
     void solve(DVec &x, DVec &b, const std::vector<double> &conv) override;
+    // full32 only: the result stays in float in x32 (zero-flagged on entry
+    // when the application starts from zero)
+    void solve_to32(DVec &x32, DVec &b, const std::vector<double> &conv);
 
   private:
     void cycle(int level, DVec &x, DVec &b, int cyc, const std::vector<double> &iconv);
@@ -99,6 +102,12 @@ class Krylov : public SolverBase {
     bool rb_merged = false;    // ... in its merged form (merged_rbicgstab.inl)
     std::unique_ptr<SolverBase> M;
     DevBuf sc;                 // scalar block (kernels.cuh Sc)
+    // an FP32 multigrid preconditioner (gpu_precond_f32 = 1, V- or W-cycles)
+    // hands its results over in float: pa32 = M^-1 p, sa32 = M^-1 s
+    bool f32io = false;        // decided at the start of every solve
+    bool f32io_ready = false;  // pa32/sa32 allocated
+    DVec pa32, sa32;
+    void enable_f32io();
     void setup() override;
     void solve(DVec &x, DVec &b, const std::vector<double> &conv) override;
     ~Krylov() override;

@@ -222,7 +222,11 @@ static uint8_t autotune(const DCsr &A, const FX *x, cudaStream_t s) {
 template <typename F, typename FX, typename I, int NV, int NRED, bool CALLER_X, typename V,
           class Epi>
 static void launch_v(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s) {
-    constexpr int VK = k::spmv_vk<FX, NV>();
+    // With dot products the grid is the canonical 1,184 blocks (one wave at
+    // eight an SM), so the threads a block has are the warps an SM keeps in
+    // flight: such kernels carry at most two right-hand sides a thread (FP32 x
+    // at four a thread measured 35 % slower on the 27-point 128^3 matrix).
+    constexpr int VK = NRED > 0 ? std::min(k::spmv_vk<FX, NV>(), 2) : k::spmv_vk<FX, NV>();
     if constexpr (NRED == 0 && NV > 1) {
         if (A.tune_on && (uintptr_t)x % (4 * sizeof(FX)) == 0) {
             int l = 0;

@@ -144,14 +144,16 @@ def fp64_transfer_params(tol):
     return p
 
 
-def vcycle_params():
+def vcycle_params(reduced=1):
     """One V(1,1) cycle of the same hierarchy as a stationary step from the
-    given x: x + M^-1 (b - A x) with the multigrid preconditioner M (FP64)."""
+    given x: x + M^-1 (b - A x) with the multigrid cycle M (levels below the
+    finest in FP32 with reduced = 1, XAMG's mg_reduced_precision)."""
     sm = {"method": "Chebyshev", "polynomial_order": 2}
     return {"solver": {"method": "MultiGrid", "max_iters": 1, "convergence_check": 0,
                        "mg_agg_num_levels": 0, "mg_strength_threshold": 0.25,
                        "mg_coarsening_type": 8, "mg_interpolation_type": 6,
-                       "mg_coarse_matrix_size": 500, "mg_reduced_precision": 0},
+                       "mg_coarse_matrix_size": 500, "mg_reduced_precision": reduced,
+                       "gpu_index_compress": 2},
             "pre_smoother": sm, "post_smoother": dict(sm),
             "coarse_grid_solver": {"method": "Direct"}}
 
@@ -196,7 +198,8 @@ def _run(n_edge, n_train, n_eval, nv, steps, level, hidden, sigma, seed, train_t
                                                     "convergence_check": 0,
                                                     "relax_factor": 0.8}}), xs, bs)
     else:
-        S_smooth = X.Solver(M, X.Params(vcycle_params()), xs, bs)
+        S_smooth = X.Solver(M, X.Params(vcycle_params(0 if smoothing == "vcycle64" else 1)),
+                            xs, bs)
     nl = S64.nlevels()
     level = min(level, nl - 1)
     LG = LearnedGuess(S64, level, hidden, seed)

@@ -307,7 +307,8 @@ class Params:
                 "mg_interpolation_type", "mg_Pmax_elements", "mg_agg_num_levels",
                 "mg_agg_interpolation_type", "mg_agg_Pmax_elements", "mg_agg_P12max_elements",
                 "gpu_precond_f32", "gpu_coarse_f64", "gpu_index_compress", "gpu_hsgs_rows",
-                "gpu_graph", "gpu_seed", "gpu_persistent", "gpu_spmv_tune", "gpu_level_bf16"}
+                "gpu_graph", "gpu_seed", "gpu_persistent", "gpu_spmv_tune", "gpu_level_bf16",
+                "gpu_solve_graph"}
 
     def __init__(self, spec=None, overrides=None, set_default=True):
         h = sz()

@@ -26,7 +26,7 @@ INT_KEYS = {"convergence_check", "convergence_info", "polynomial_order", "max_it
 # (index storage, graphs, launch tuning, the setup's seed, the GPU's
 # Gauss-Seidel block size); any other extension key has no reference meaning
 NEUTRAL_EXT_KEYS = {"gpu_index_compress", "gpu_graph", "gpu_spmv_tune", "gpu_seed",
-                    "gpu_hsgs_rows", "gpu_persistent"}
+                    "gpu_hsgs_rows", "gpu_persistent", "gpu_solve_graph"}
 _libs = {}
 sz = C.c_size_t
 
