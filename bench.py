@@ -311,6 +311,9 @@ def roofline(X, torch, stream, S, n, nv, args, which=3, reps=50):
     A0 = S.level_csr(0, which)
     esz = 4 if A0.val_f32 else 8                    # x and y elements
     vsz = {0: 8, 1: 4, 2: 2}[A0.val_f32]             # stored values (2: BF16)
+    # a grid-stencil copy (gpu_index_compress = 3) is what the SpMV reads:
+    # one value per slot and row, a 4-byte entry mask per row, no columns
+    st_pat = S.level_stencil(0, which)[0]
     dt = torch.float32 if A0.val_f32 else torch.float64
     xd = torch.empty(n * nv, dtype=dt, device="cuda").uniform_(-1, 1)
     yd = torch.empty(n * nv, dtype=dt, device="cuda")
@@ -325,15 +328,24 @@ def roofline(X, torch, stream, S, n, nv, args, which=3, reps=50):
         e1.record(stream)
     e1.synchronize()
     ms = e0.elapsed_time(e1) / reps
-    alg = A0.nnz * (vsz + abs(A0.col_bytes)) + (n + 1) * 4 + 2 * n * nv * esz
+    fname = "float" if esz == 4 else "double"
+    if st_pat >= 0:
+        slots = 27 if st_pat == 0 else 7
+        alg = slots * n * vsz + n * 4 + 2 * n * nv * esz
+        kname = f"k_spmv_stencil<{fname}> level 0, EStore, nv={nv}, " \
+                f"{slots}-slot grid stencil" + (", BF16 values" if vsz == 2 else "")
+        tkey = f"{args.workload}_n{n}_which{which}_nv{nv}_v{vsz}_st{slots}"
+    else:
+        alg = A0.nnz * (vsz + abs(A0.col_bytes)) + (n + 1) * 4 + 2 * n * nv * esz
+        kname = f"k_spmv<{fname}> level 0, EStore, nv={nv}, " \
+                f"col_bytes={A0.col_bytes}" + (", BF16 values" if vsz == 2 else "")
+        tkey = f"{args.workload}_n{n}_which{which}_nv{nv}_v{vsz}"
     achieved = alg / (ms * 1e-3) / 1e9
     peak, peak_kind = peaks()
-    kname = f"k_spmv<{'float' if esz == 4 else 'double'}> level 0, EStore, nv={nv}, " \
-            f"col_bytes={A0.col_bytes}" + (", BF16 values" if vsz == 2 else "")
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "spmv_traffic.json")
     if os.path.exists(tfile):
-        t = json.load(open(tfile)).get(f"{args.workload}_n{n}_which{which}_nv{nv}_v{vsz}")
+        t = json.load(open(tfile)).get(tkey)
         if t:
             traffic = t["dram_bytes_per_launch"]
     return {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,

@@ -144,6 +144,24 @@ int XAMG_b200_solver_level_info(size_t sid, int level, int which, uint64_t *nrow
  * are tuned; every shape gives the same results bit for bit. */
 int XAMG_b200_solver_level_tuned(size_t sid, int level, int which, uint8_t *codes);
 
+/* Grid-stencil storage (parameter gpu_index_compress = 3; no counterpart in
+ * the reference, whose CSR blocks always carry column indices). A square
+ * matrix whose entries all lie on the offsets dz*S2 + dy*S + dx (|dz|, |dy|,
+ * |dx| <= 1) of a 27-point box (pattern 0) or a 7-point star (pattern 1) is
+ * also stored without column indices: one value array per stencil slot and
+ * a bit mask of the entries each row has. The SpMVs without dot products then
+ * read that copy and sum each row in the CSR order, so results are unchanged
+ * bit for bit. Rows must all be sorted by column, or all store their
+ * diagonal first and the rest sorted (*diag_first = 1).
+ * XAMG_b200_stencil_layout runs the detection on host CSR arrays (no GPU):
+ * *pattern = -1 where the matrix does not qualify.
+ * XAMG_b200_solver_level_stencil reports a level matrix's copy (pattern -1:
+ * none). */
+int XAMG_b200_stencil_layout(uint64_t nrows, const uint32_t *row, const uint32_t *col,
+                             int *pattern, uint32_t *S, uint32_t *S2, int *diag_first);
+int XAMG_b200_solver_level_stencil(size_t sid, int level, int which, int *pattern, uint32_t *S,
+                                   uint32_t *S2, int *diag_first);
+
 /* Copy level matrix `which` back from the device exactly as stored: row
  * pointers (u32), narrowed columns (col_bytes each), values (float/double). */
 int XAMG_b200_solver_level_download(size_t sid, int level, int which, uint32_t *row, void *col,

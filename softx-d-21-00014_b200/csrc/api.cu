@@ -875,6 +875,38 @@ int XAMG_b200_solver_level_info(size_t sid, int level, int which, uint64_t *nrow
     });
 }
 
+int XAMG_b200_stencil_layout(uint64_t nrows, const uint32_t *row, const uint32_t *col,
+                             int *pattern, uint32_t *S, uint32_t *S2, int *diag_first) {
+    return guarded([&] {
+        XG_REQUIRE(row && col && pattern && S && S2 && diag_first, XAMG_ERR_INVALID_ARG,
+                   "null array");
+        HCsr h;
+        h.nrows = h.ncols = nrows;
+        h.row.assign(row, row + nrows + 1);
+        h.col.assign(col, col + h.row[nrows]);
+        h.val.assign(h.col.size(), 0.0);
+        int pat = -1;
+        uint32_t s1 = 0, s2 = 0;
+        bool df = false;
+        if (!stencil_layout(h, pat, s1, s2, df)) pat = -1;
+        *pattern = pat;
+        *S = s1;
+        *S2 = s2;
+        *diag_first = df ? 1 : 0;
+    });
+}
+
+int XAMG_b200_solver_level_stencil(size_t sid, int level, int which, int *pattern, uint32_t *S,
+                                   uint32_t *S2, int *diag_first) {
+    return guarded([&] {
+        const DCsr &d = level_matrix(sid, level, which);
+        if (pattern) *pattern = d.st_pat;
+        if (S) *S = d.st_S;
+        if (S2) *S2 = d.st_S2;
+        if (diag_first) *diag_first = d.st_diag_first ? 1 : 0;
+    });
+}
+
 int XAMG_b200_solver_level_tuned(size_t sid, int level, int which, uint8_t *codes) {
     return guarded([&] {
         XG_REQUIRE(codes, XAMG_ERR_INVALID_ARG, "null array");

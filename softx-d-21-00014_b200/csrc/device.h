@@ -144,6 +144,14 @@ struct DCsr {
     // 2 sixteen)
     bool tune_on = false;
     mutable uint8_t tuned[2][2][6] = {};
+    // Grid-stencil copy (gpu_index_compress = 3, csrc/stencil.cuh): the slot
+    // pattern (-1: none, else k::ST_BOX27 or k::ST_STAR7), the line and plane
+    // strides, the row order, the [slots][nrows] values in the CSR values'
+    // type and the per-row entry masks. The SpMVs without dot products use it.
+    int st_pat = -1;
+    uint32_t st_S = 0, st_S2 = 0;
+    bool st_diag_first = false;  // rows store their diagonal first
+    DevBuf st_val, st_mask;
 
     template <typename F>
     k::CsrArgs<F> args() const {
@@ -158,7 +166,8 @@ struct DCsr {
 // narrow: 0 keeps 32-bit columns; 1 applies XAMG's rule; 2 additionally
 // stores signed 16-bit offsets col - row (col_bytes = -2) for square
 // matrices whose columns need more than 16 bits but whose entries all lie
-// within 32767 of the diagonal.
+// within 32767 of the diagonal; 3 also adds the grid-stencil copy where the
+// matrix has that structure (stencil_layout).
 // tune: let the SpMVs without dot products on this matrix pick their launch
 // shape by measurement (gpu_spmv_tune).
 // bf16 (with f32): store the values rounded to float and then to BF16
@@ -166,6 +175,14 @@ struct DCsr {
 void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s, int tune = 0,
                 bool bf16 = false);
 void download_csr(const DCsr &d, uint32_t *row, void *col, void *val);
+
+// Whether a square CSR block has the grid-stencil structure of
+// csrc/stencil.cuh: every row sorted by column (or every row with its
+// diagonal first and the rest sorted: diag_first), every offset col - row
+// equal to dz*S2 + dy*S + dx (|dz|, |dy|, |dx| <= 1) with a slot in the
+// pattern, S >= 3 and S2 >= 2S + 3 (so that ascending offsets are ascending
+// (dz, dy, dx)). Sets the pattern, strides and order.
+bool stencil_layout(const HCsr &h, int &pat, uint32_t &S, uint32_t &S2, bool &diag_first);
 
 template <typename T>
 void upload(DevBuf &b, const std::vector<T> &v, cudaStream_t s) {

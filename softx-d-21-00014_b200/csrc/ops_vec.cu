@@ -4,6 +4,7 @@
 #include <cstring>
 
 #include "ops.h"
+#include "stencil.cuh"
 
 namespace xg {
 
@@ -229,6 +230,159 @@ template void axpy_k<float>(float *, const float *, const double *, uint64_t, in
 // CSR upload with XAMG's narrowing (matrix_block::assemble, matrix.h:78-93:
 // hash from encode_hash, values converted to float when reduced).
 // ---------------------------------------------------------------------------
+// (dz, dy, dx) of offset `off` for strides S, S2 (S >= 3, S2 >= 2S + 3: the
+// nearest multiple of S2, then of S, is unique); false if a part exceeds 1.
+static bool stencil_split(int64_t off, int64_t S, int64_t S2, int &dz, int &dy, int &dx) {
+    auto nearest = [](int64_t a, int64_t q) {  // a/q rounded to the nearest
+        return a >= 0 ? (a + q / 2) / q : -((-a + q / 2) / q);
+    };
+    const int64_t z = nearest(off, S2), rz = off - z * S2;
+    const int64_t y = nearest(rz, S), rx = rz - y * S;
+    if (z < -1 || z > 1 || y < -1 || y > 1 || rx < -1 || rx > 1) return false;
+    dz = (int)z;
+    dy = (int)y;
+    dx = (int)rx;
+    return true;
+}
+
+static int stencil_slot(int pat, int dz, int dy, int dx) {
+    return pat == k::ST_BOX27 ? k::st_slot<k::ST_BOX27>(dz, dy, dx)
+                              : k::st_slot<k::ST_STAR7>(dz, dy, dx);
+}
+
+// Slot of an offset for a pattern and strides (-1: none), remembering the
+// offsets seen (at most 27 distinct ones in a matrix that qualifies).
+struct SlotCache {
+    int pat;
+    int64_t S, S2;
+    std::vector<std::pair<int64_t, int>> seen;  // sorted by offset
+    int operator()(int64_t off) {
+        auto it = std::lower_bound(seen.begin(), seen.end(), std::make_pair(off, -2));
+        if (it != seen.end() && it->first == off) return it->second;
+        int dz, dy, dx, sl = -1;
+        if (stencil_split(off, S, S2, dz, dy, dx)) sl = stencil_slot(pat, dz, dy, dx);
+        seen.insert(it, std::make_pair(off, sl));
+        return sl;
+    }
+};
+
+// Row order of a CSR block: bit 0 set if every row is sorted by column, bit 1
+// if every row has its diagonal (where present) first and the rest sorted.
+static int row_orders(const HCsr &h) {
+    bool sorted = true, dfirst = true;
+    for (uint64_t i = 0; i < h.nrows && (sorted || dfirst); ++i) {
+        const uint64_t a = h.row[i], e = h.row[i + 1];
+        for (uint64_t j = a + 1; j < e; ++j)
+            if (h.col[j] <= h.col[j - 1]) sorted = false;
+        const uint64_t s = (a < e && h.col[a] == i) ? a + 1 : a;
+        for (uint64_t j = s; j < e; ++j) {
+            if (h.col[j] == i) dfirst = false;  // a diagonal that is not first
+            if (j > s && h.col[j] <= h.col[j - 1]) dfirst = false;
+        }
+    }
+    return (sorted ? 1 : 0) | (dfirst ? 2 : 0);
+}
+
+bool stencil_layout(const HCsr &h, int &pat, uint32_t &S, uint32_t &S2, bool &diag_first) {
+    const uint64_t n = h.nrows;
+    if (h.ncols != n || n < 27 || h.nnz() == 0 || n > UINT32_MAX / 32) return false;
+    // the offsets of a run of rows in the middle of the matrix (interior
+    // rows of a grid) give the candidate strides
+    std::vector<int64_t> offs;
+    const uint64_t r0 = n / 2, r1 = std::min<uint64_t>(n, r0 + 4096);
+    for (uint64_t i = r0; i < r1; ++i)
+        for (uint64_t j = h.row[i]; j < h.row[i + 1]; ++j) {
+            const int64_t o = (int64_t)h.col[j] - (int64_t)i;
+            if (std::find(offs.begin(), offs.end(), o) == offs.end()) {
+                if (offs.size() == 27) return false;
+                offs.push_back(o);
+            }
+        }
+    std::vector<int64_t> pos;
+    for (int64_t o : offs)
+        if (o > 0) pos.push_back(o);
+    std::sort(pos.begin(), pos.end());
+    // candidate strides: the second-smallest positive offset is S - 1 (box)
+    // or S (star); the smallest one beyond S + 1 is S2 - S - 1, S2 - S,
+    // S2 - 1 or S2. Any decomposition that covers every offset computes the
+    // right columns; the star pattern (fewer slots) is preferred.
+    struct Cand {
+        int pat;
+        int64_t S, S2;
+    };
+    std::vector<Cand> cands;
+    if (pos.size() >= 3) {
+        for (int p : {k::ST_STAR7, k::ST_BOX27})
+            for (int64_t s1 : {pos[1], pos[1] + 1}) {
+                auto it = std::upper_bound(pos.begin(), pos.end(), s1 + 1);
+                if (it == pos.end()) continue;
+                for (int64_t d : {(int64_t)0, (int64_t)1, s1, s1 + 1})
+                    cands.push_back({p, s1, *it + d});
+            }
+    }
+    for (const Cand &c : cands) {
+        if (c.S < 3 || c.S2 < 2 * c.S + 3 || c.S2 >= (int64_t)n) continue;
+        SlotCache slot{c.pat, c.S, c.S2, {}};
+        bool ok = true;
+        for (uint64_t i = 0; i < n && ok; ++i)
+            for (uint64_t j = h.row[i]; j < h.row[i + 1]; ++j) {
+                if (slot((int64_t)h.col[j] - (int64_t)i) < 0) {
+                    ok = false;
+                    break;
+                }
+            }
+        if (ok) {
+            const int ord = row_orders(h);
+            if (ord == 0) return false;
+            pat = c.pat;
+            S = (uint32_t)c.S;
+            S2 = (uint32_t)c.S2;
+            diag_first = (ord & 1) == 0;
+            return true;
+        }
+    }
+    return false;
+}
+
+// The grid-stencil copy of `h` (values in the type d stores: double, float
+// or BF16 rounded from float), where the matrix has that structure.
+static void upload_stencil(const HCsr &h, DCsr &d, cudaStream_t s) {
+    int pat;
+    uint32_t S, S2;
+    bool df;
+    if (!stencil_layout(h, pat, S, S2, df)) return;
+    const uint64_t n = h.nrows;
+    const int K = pat == k::ST_BOX27 ? k::st_slots<k::ST_BOX27>() : k::st_slots<k::ST_STAR7>();
+    std::vector<uint32_t> mask(n, 0u);
+    std::vector<double> v((size_t)K * n, 0.0);
+    SlotCache slot{pat, S, S2, {}};
+    for (uint64_t i = 0; i < n; ++i)
+        for (uint64_t j = h.row[i]; j < h.row[i + 1]; ++j) {
+            const int sl = slot((int64_t)h.col[j] - (int64_t)i);
+            mask[i] |= 1u << sl;
+            v[(size_t)sl * n + i] = h.val[j];
+        }
+    upload(d.st_mask, mask, s);
+    if (d.bf16) {
+        std::vector<__nv_bfloat16> w(v.size());
+        for (size_t e = 0; e < v.size(); ++e) w[e] = __float2bfloat16_rn((float)v[e]);
+        upload(d.st_val, w, s);
+        XG_CUDA(cudaStreamSynchronize(s));
+    } else if (d.f32) {
+        std::vector<float> w(v.size());
+        for (size_t e = 0; e < v.size(); ++e) w[e] = (float)v[e];
+        upload(d.st_val, w, s);
+        XG_CUDA(cudaStreamSynchronize(s));
+    } else {
+        upload(d.st_val, v, s);
+    }
+    XG_CUDA(cudaStreamSynchronize(s));
+    d.st_pat = pat;
+    d.st_S = S;
+    d.st_S2 = S2;
+    d.st_diag_first = df;
+}
+
 void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s, int tune,
                 bool bf16) {
     d.tune_on = tune != 0;
@@ -295,6 +449,10 @@ void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s, in
     } else {
         upload(d.val, h.val, s);
     }
+    d.st_pat = -1;
+    d.st_val.release();
+    d.st_mask.release();
+    if (narrow >= 3) upload_stencil(h, d, s);
     XG_CUDA(cudaStreamSynchronize(s));
 }
 

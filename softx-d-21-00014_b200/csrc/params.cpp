@@ -73,7 +73,7 @@ static const std::map<std::string, KeyInfo> &dictionary() {
         {"mg_agg_P12max_elements", {'I', "MultiGrid", "0", "inf", ""}},
         {"gpu_precond_f32", {'I', "", "0", "1", ""}},
         {"gpu_coarse_f64", {'I', "", "0", "1", ""}},
-        {"gpu_index_compress", {'I', "", "0", "2", ""}},
+        {"gpu_index_compress", {'I', "", "0", "3", ""}},
         {"gpu_hsgs_rows", {'I', "", "1", "inf", ""}},
         {"gpu_graph", {'I', "", "0", "1", ""}},
         {"gpu_spmv_tune", {'I', "", "0", "1", ""}},

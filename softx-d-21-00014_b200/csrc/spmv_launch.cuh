@@ -9,6 +9,7 @@
 #include <type_traits>
 
 #include "ops.h"
+#include "stencil.cuh"
 
 namespace xg {
 namespace ops {
@@ -257,12 +258,52 @@ static void launch_v(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s)
     }
 }
 
+// The grid-stencil kernel (csrc/stencil.cuh) on a matrix's stencil copy: M
+// grid lines a thread, as many right-hand sides a thread as the CSR kernel
+// carries, one thread per (group of M lines, position in the line,
+// right-hand-side group).
+constexpr int ST_LINES = 4;
+template <typename F, int NV, typename V, class Epi>
+static void launch_stencil(const DCsr &A, const F *x, const Epi &epi, cudaStream_t s) {
+    constexpr int VK = k::spmv_vk<F, NV>();
+    constexpr int M = ST_LINES;
+    XG_REQUIRE(A.nrows * (uint64_t)NV < (1ull << 32), XAMG_ERR_UNSUPPORTED,
+               "SpMV: x of 2^32 or more values");
+    const uint64_t groups = (A.nrows + (uint64_t)M * A.st_S - 1) / ((uint64_t)M * A.st_S);
+    const uint64_t threads = groups * A.st_S * (NV / VK);
+    const uint64_t blocks = (threads + k::ST_THREADS - 1) / k::ST_THREADS;
+    const k::StencilArgs a{A.st_val.p, A.st_mask.as<uint32_t>(), (uint32_t)A.nrows, A.st_S,
+                           A.st_S2, A.st_diag_first ? 1 : 0};
+    if (A.st_pat == k::ST_BOX27)
+        k::k_spmv_stencil<F, F, NV, VK, M, k::ST_BOX27, Epi, V>
+            <<<(unsigned)blocks, k::ST_THREADS, 0, s>>>(a, x, epi);
+    else
+        k::k_spmv_stencil<F, F, NV, VK, M, k::ST_STAR7, Epi, V>
+            <<<(unsigned)blocks, k::ST_THREADS, 0, s>>>(a, x, epi);
+    XG_CUDA(cudaGetLastError());
+    ++g_kernel_launches;
+}
+
 // FP32 matrices may store their values in BF16 (DCsr::bf16; gpu_level_bf16):
-// the kernel then widens each value to float as it reads it.
+// the kernel then widens each value to float as it reads it. SpMVs without
+// dot products on a matrix with a grid-stencil copy run the stencil kernel
+// (the same sums).
 template <typename F, typename FX, typename I, int NV, int NRED, bool CALLER_X = false,
           class Epi>
 static void launch(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s) {
     if (A.nrows == 0) return;
+    if constexpr (NRED == 0 && std::is_same<F, FX>::value) {
+        constexpr uintptr_t SA = k::spmv_vk<F, NV>() * sizeof(F);
+        if (A.st_pat >= 0 && (!CALLER_X || (uintptr_t)x % SA == 0)) {
+            if constexpr (std::is_same<F, float>::value)
+                if (A.bf16) {
+                    launch_stencil<F, NV, __nv_bfloat16>(A, x, epi, s);
+                    return;
+                }
+            launch_stencil<F, NV, F>(A, x, epi, s);
+            return;
+        }
+    }
     if constexpr (std::is_same<F, float>::value && std::is_same<FX, float>::value) {
         if (A.bf16) {
             launch_v<F, FX, I, NV, NRED, CALLER_X, __nv_bfloat16>(A, x, epi, s);

@@ -61,7 +61,7 @@ EXT_SYMBOLS = [
     "XAMG_b200_matrix_hierarchy_load", "XAMG_b200_gemm_bf16", "XAMG_b200_mlp_create",
     "XAMG_b200_mlp_destroy", "XAMG_b200_mlp_predict", "XAMG_b200_mlp_train_step",
     "XAMG_b200_mlp_gradients", "XAMG_b200_mlp_params", "XAMG_b200_solver_solve_batch",
-    "XAMG_b200_solver_level_tuned",
+    "XAMG_b200_solver_level_tuned", "XAMG_b200_stencil_layout", "XAMG_b200_solver_level_stencil",
 ]
 
 
@@ -201,6 +201,12 @@ def lib():
         "XAMG_b200_matrix_hierarchy_load": (C.c_int, [C.c_size_t, C.c_char_p]),
         "XAMG_b200_solver_solve_batch": (C.c_int, [C.c_int, vp, vp, vp, vp]),
         "XAMG_b200_solver_level_tuned": (C.c_int, [C.c_size_t, C.c_int, C.c_int, vp]),
+        "XAMG_b200_stencil_layout": (C.c_int, [u64, vp, vp, C.POINTER(C.c_int),
+                                               C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                               C.POINTER(C.c_int)]),
+        "XAMG_b200_solver_level_stencil": (C.c_int, [C.c_size_t, C.c_int, C.c_int,
+                                                     C.POINTER(C.c_int), C.POINTER(C.c_uint32),
+                                                     C.POINTER(C.c_uint32), C.POINTER(C.c_int)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -260,6 +266,17 @@ def write_system(path, row, col, val, nv=1, b=None, x=None):
     call("XAMG_b200_write_system", str(path).encode(), len(row) - 1, len(col), _ptr(row),
          _ptr(col), _ptr(val), nv, None if bb is None else _ptr(bb),
          None if xx is None else _ptr(xx))
+
+
+def stencil_layout(row, col):
+    """Grid-stencil detection on host CSR arrays (no GPU): (pattern, S, S2,
+    diag_first), pattern -1 where the matrix does not qualify."""
+    row = np.ascontiguousarray(row, np.uint32)
+    col = np.ascontiguousarray(col, np.uint32)
+    pat, S, S2, df = C.c_int(), C.c_uint32(), C.c_uint32(), C.c_int()
+    call("XAMG_b200_stencil_layout", len(row) - 1, _ptr(row), _ptr(col), C.byref(pat),
+         C.byref(S), C.byref(S2), C.byref(df))
+    return pat.value, S.value, S2.value, df.value
 
 
 def generate_cube(nx, ny, nz):
@@ -515,6 +532,14 @@ class Solver:
         out = np.zeros(24, np.uint8)
         call("XAMG_b200_solver_level_tuned", self.h, level, which, _ptr(out))
         return out.reshape(2, 2, 6)
+
+    def level_stencil(self, level, which):
+        """The level matrix's grid-stencil copy: (pattern, S, S2, diag_first),
+        pattern -1 where it has none."""
+        pat, S, S2, df = C.c_int(), C.c_uint32(), C.c_uint32(), C.c_int()
+        call("XAMG_b200_solver_level_stencil", self.h, level, which, C.byref(pat), C.byref(S),
+             C.byref(S2), C.byref(df))
+        return pat.value, S.value, S2.value, df.value
 
     def level_download(self, level, which):
         info = self.level_info(level, which)

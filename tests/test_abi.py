@@ -154,7 +154,7 @@ def test_param_ranges_and_allowed_sets(xamg):
            ("preconditioner", "mg_coarse_matrix_size", 2001),
            ("preconditioner", "mg_strength_threshold", -0.1),
            ("preconditioner", "mg_agg_interpolation_type", 0), ("solver", "rel_tolerance", -1e-8),
-           ("solver", "convergence_check", 2), ("preconditioner", "gpu_index_compress", 3)]
+           ("solver", "convergence_check", 2), ("preconditioner", "gpu_index_compress", 4)]
     for role, key, value in bad:
         with pytest.raises(xamg.XamgError) as e:
             p.add(role, key, value)
@@ -165,7 +165,7 @@ def test_param_ranges_and_allowed_sets(xamg):
             ("pre_smoother", "spectrum_fraction", 1.0), ("preconditioner", "mg_cycle", 2),
             ("preconditioner", "mg_coarsening_type", 22), ("preconditioner", "mg_max_levels", 50),
             ("preconditioner", "mg_coarse_matrix_size", 2000), ("solver", "max_iters", 65535),
-            ("preconditioner", "gpu_index_compress", 2)]
+            ("preconditioner", "gpu_index_compress", 3)]
     for role, key, value in good:
         p.add(role, key, value)
     p.change("preconditioner", "mg_cycle", 1)
