@@ -141,7 +141,7 @@ struct DCsr {
     // [value type is float][x type is float][log2 nv]: 0 = not tuned yet,
     // else 1 + 9 * (right-hand sides a thread: 0 default, 1 alternative) +
     // 3 * (staging: 0 one buffer, 1 two, 2 none) + (tile run: 0 one, 1 four,
-    // 2 sixteen)
+    // 2 sixteen), or 19: the warp-per-row kernel (k_spmv_wide)
     bool tune_on = false;
     mutable uint8_t tuned[2][2][6] = {};
     // Grid-stencil copy (gpu_index_compress = 3, csrc/stencil.cuh): the slot
@@ -152,6 +152,12 @@ struct DCsr {
     uint32_t st_S = 0, st_S2 = 0;
     bool st_diag_first = false;  // rows store their diagonal first
     DevBuf st_val, st_mask;
+    // with tuning on: the kernel measured fastest for the SpMVs without dot
+    // products, per [value type is float][log2 nv]: 0 = not tuned yet, 1 the
+    // stencil kernel with 64 registers a thread, 2 with 128, 3 the CSR kernel
+    mutable uint8_t st_choice[2][6] = {};
+    uint8_t st_force = 0;     // gpu_spmv_tune = 2: always the 128-register form
+    bool wide_force = false;  // gpu_spmv_tune = 3: the warp-per-row kernel where allowed
 
     template <typename F>
     k::CsrArgs<F> args() const {
@@ -169,7 +175,10 @@ struct DCsr {
 // within 32767 of the diagonal; 3 also adds the grid-stencil copy where the
 // matrix has that structure (stencil_layout).
 // tune: let the SpMVs without dot products on this matrix pick their launch
-// shape by measurement (gpu_spmv_tune).
+// shape by measurement (gpu_spmv_tune = 1); 2: no measurement, the stencil
+// copy's SpMVs use the 128-register form; 3: no measurement, SpMVs without
+// dot products on matrices of at most 2^20 rows times nv use the
+// warp-per-row kernel.
 // bf16 (with f32): store the values rounded to float and then to BF16
 // (round to nearest even), the arithmetic staying in float.
 void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s, int tune = 0,

@@ -536,6 +536,54 @@ __global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
     if constexpr (NRED > 0) canon_final<F, NV, NRED, CT / VK>(ra, B, epi);
 }
 
+// Warp-per-row SpMV for matrices with few rows (the coarse levels and their
+// transfers), where k_spmv's time is one thread's chain of gathers down a
+// whole row. A warp takes one row at a time: its lanes gather the products
+// of 32/NV entries at once (lane = entry slot * NV + right-hand side), each
+// product rounded on its own (mul(x, a), as row_sum rounds it), into a
+// shared-memory chunk of WCH entries; then lane k < NV adds the chunk's
+// products to its sum in entry order. So every output element is the same
+// sequence of separately rounded products and sums as in k_spmv, while a
+// row's gathers are in flight together.
+constexpr int WT = 256;  // threads per block (8 warps)
+template <int NV>
+constexpr int wide_chunk() { return 512 / NV; }  // entries per warp-chunk
+template <typename F, typename FX, typename I, int NV, class Epi, typename V = F>
+__global__ void __launch_bounds__(WT) k_spmv_wide(CsrArgs<F> A, const FX *__restrict__ x, Epi epi) {
+    constexpr int E = NV >= 32 ? 1 : 32 / NV;  // entries a warp gathers per round
+    constexpr int CH = wide_chunk<NV>();
+    __shared__ F prod[WT / 32][CH * NV];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int k = lane % NV, es = lane / NV;  // es < E for NV <= 32
+    const uint32_t *__restrict__ row = A.row;
+    const I *__restrict__ col = (const I *)A.col;
+    const V *__restrict__ val = (const V *)A.val;
+    F *pw = prod[warp];
+    const uint64_t nw = (uint64_t)gridDim.x * (WT / 32);
+    for (uint64_t i = (uint64_t)blockIdx.x * (WT / 32) + warp; i < A.n; i += nw) {
+        const uint32_t j0 = __ldg(&row[i]), j1 = __ldg(&row[i + 1]);
+        const uint32_t i32 = (uint32_t)i;
+        F y = k < NV && lane < NV ? epi.init(i, k) : F(0);
+        for (uint32_t c0 = j0; c0 < j1; c0 += CH) {
+            const uint32_t len = j1 - c0 < (uint32_t)CH ? j1 - c0 : (uint32_t)CH;
+#pragma unroll 4
+            for (uint32_t e = es; e < len; e += E) {
+                const uint32_t c = col_at32<I>(__ldg(&col[c0 + e]), i32);
+                const F av = val_as<F, V>(__ldg(&val[c0 + e]));
+                pw[e * NV + k] = mul((F)__ldg(&x[c * (uint32_t)NV + (uint32_t)k]), av);
+            }
+            __syncwarp();
+            if (lane < NV) {
+#pragma unroll 8
+                for (uint32_t e = 0; e < len; ++e) y = add(y, pw[e * NV + lane]);
+            }
+            __syncwarp();
+        }
+        F none[1] = {F(0)};
+        if (lane < NV) epi.store(i, lane, y, none);
+    }
+}
+
 // Bounded-wait check: one block waits on an mbarrier that nothing arrives
 // at, gives up after limit_ns and raises the timeout flag, as a staging wait
 // of k_spmv does when its copy never lands. Nothing is in flight when it

@@ -385,7 +385,9 @@ static void upload_stencil(const HCsr &h, DCsr &d, cudaStream_t s) {
 
 void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s, int tune,
                 bool bf16) {
-    d.tune_on = tune != 0;
+    d.tune_on = tune == 1;
+    d.st_force = tune == 2 ? 2 : 0;
+    d.wide_force = tune == 3;
     d.bf16 = f32 && bf16;
     d.nrows = h.nrows;
     d.ncols = h.ncols;

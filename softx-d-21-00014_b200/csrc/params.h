@@ -82,7 +82,9 @@ struct SolverCfg {
     int gpu_index_compress = 1; // XAMG narrowing of column indices on upload
     int gpu_hsgs_rows = 32;     // target rows per hybrid Gauss-Seidel block
     int gpu_graph = 1;          // replay preconditioner applications as CUDA graphs
-    int gpu_spmv_tune = 1;      // SpMV launch shapes picked by measurement
+    int gpu_spmv_tune = 1;      // SpMV launch shapes picked by measurement (2: no tuning,
+                                // the grid-stencil kernel's 128-register form; 3: no
+                                // tuning, the warp-per-row kernel on small matrices)
     int gpu_level_bf16 = 0;     // finest FP32 cycle levels whose matrix values are BF16
     int gpu_seed = 0;           // seed of the host setup's random choices
     int gpu_persistent = 1;     // eligible BiCGStab solves in one cooperative launch

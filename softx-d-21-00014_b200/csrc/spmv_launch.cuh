@@ -140,6 +140,22 @@ static void launch_vk(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s
     ++g_kernel_launches;
 }
 
+// The warp-per-row kernel (k_spmv_wide): one wave of 256-thread blocks.
+template <typename F, typename FX, typename I, int NV, typename V, class Epi>
+static void launch_wide(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s) {
+    XG_REQUIRE(std::max(A.ncols, A.nrows) * (uint64_t)NV < (1ull << 32), XAMG_ERR_UNSUPPORTED,
+               "SpMV: x of 2^32 or more values");
+    auto kern = k::k_spmv_wide<F, FX, I, NV, Epi, V>;
+    const int res = resident_blocks(kern, k::WT, 0);
+    const uint64_t need = (A.nrows + k::WT / 32 - 1) / (k::WT / 32);
+    const uint32_t P = (uint32_t)std::min<uint64_t>(need, (uint64_t)res * ctx().sms);
+    kern<<<P, k::WT, 0, s>>>(A.args<F>(), x, epi);
+    XG_CUDA(cudaGetLastError());
+    ++g_kernel_launches;
+}
+constexpr uint8_t TUNE_WIDE = 19;         // autotuner code of the warp-per-row kernel
+constexpr uint64_t WIDE_MAX_VALUES = 1u << 20;  // rows * nv up to which it is a candidate
+
 // Autotuner of the SpMVs without dot products: the right-hand sides a thread
 // carries (2 or 4; the alternative of spmv_vk's choice), the staging buffers
 // (1, 2, or none: tiles read from global memory, for small matrices where the
@@ -147,9 +163,10 @@ static void launch_vk(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s
 // takes (1, 4 or 16) are
 // timed with CUDA events on the caller's x into a scratch y (EStore), once
 // per matrix, precision and nv, outside any graph capture; the fastest is
-// kept in the matrix (DCsr::tuned). Every candidate sums each (row,
-// right-hand side) in the same CSR order, so the choice never changes a
-// result.
+// kept in the matrix (DCsr::tuned). Matrices of at most WIDE_MAX_VALUES rows
+// times nv also time the warp-per-row kernel (code TUNE_WIDE). Every candidate
+// sums each (row, right-hand side) in the same CSR order, so the choice never
+// changes a result.
 constexpr uint32_t TUNE_RUNS[3] = {1, 4, 16};
 struct Tuned {
     int alt;
@@ -206,6 +223,24 @@ static uint8_t autotune(const DCsr &A, const FX *x, cudaStream_t s) {
                     code = (uint8_t)(1 + alt * 9 + (nb - 1) * 3 + ri);
                 }
             }
+    if (A.nrows * (uint64_t)NV <= WIDE_MAX_VALUES) {
+        auto go = [&] { launch_wide<F, FX, I, NV, V>(A, x, e, s); };
+        float ms = 1e30f;
+        go();
+        for (int round = 0; round < 2; ++round) {
+            XG_CUDA(cudaEventRecord(e0, s));
+            for (int r = 0; r < 3; ++r) go();
+            XG_CUDA(cudaEventRecord(e1, s));
+            XG_CUDA(cudaEventSynchronize(e1));
+            float t = 0;
+            XG_CUDA(cudaEventElapsedTime(&t, e0, e1));
+            ms = std::min(ms, t);
+        }
+        if (ms < best) {
+            best = ms;
+            code = TUNE_WIDE;
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     XG_CUDA(cudaStreamSynchronize(s));
@@ -228,12 +263,22 @@ static void launch_v(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s)
     // flight: such kernels carry at most two right-hand sides a thread (FP32 x
     // at four a thread measured 35 % slower on the 27-point 128^3 matrix).
     constexpr int VK = NRED > 0 ? std::min(k::spmv_vk<FX, NV>(), 2) : k::spmv_vk<FX, NV>();
+    if constexpr (NRED == 0) {
+        if (A.wide_force && A.nrows * (uint64_t)NV <= WIDE_MAX_VALUES) {
+            launch_wide<F, FX, I, NV, V>(A, x, epi, s);
+            return;
+        }
+    }
     if constexpr (NRED == 0 && NV > 1) {
         if (A.tune_on && (uintptr_t)x % (4 * sizeof(FX)) == 0) {
             int l = 0;
             while ((1 << l) < NV) ++l;
             uint8_t &t = A.tuned[sizeof(F) == 4][sizeof(FX) == 4][l];
             if (!t) t = autotune<F, FX, I, NV, V>(A, x, s);
+            if (t == TUNE_WIDE) {
+                launch_wide<F, FX, I, NV, V>(A, x, epi, s);
+                return;
+            }
             if (t) {
                 const Tuned c = tuned_shape(t);
                 if (c.alt)
@@ -260,34 +305,118 @@ static void launch_v(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s)
 
 // The grid-stencil kernel (csrc/stencil.cuh) on a matrix's stencil copy: M
 // grid lines a thread, as many right-hand sides a thread as the CSR kernel
-// carries, one thread per (group of M lines, position in the line,
-// right-hand-side group).
+// carries; one wave of persistent blocks over the tiles, two staging buffers
+// a block unless that lowers the resident blocks.
 constexpr int ST_LINES = 4;
-template <typename F, int NV, typename V, class Epi>
-static void launch_stencil(const DCsr &A, const F *x, const Epi &epi, cudaStream_t s) {
+template <typename F, int NV, typename V, int PAT, int MINB, class Epi>
+static void launch_stencil_p(const DCsr &A, const F *x, const Epi &epi, cudaStream_t s) {
     constexpr int VK = k::spmv_vk<F, NV>();
+    constexpr int G = NV / VK;
     constexpr int M = ST_LINES;
+    constexpr uint32_t TX = k::ST_THREADS / G;
+    constexpr uint32_t BUF = k::st_buffer_bytes<V, G, M, PAT>();
     XG_REQUIRE(A.nrows * (uint64_t)NV < (1ull << 32), XAMG_ERR_UNSUPPORTED,
                "SpMV: x of 2^32 or more values");
+    auto kern = k::k_spmv_stencil<F, F, NV, VK, M, PAT, MINB, Epi, V>;
+    static bool big_smem = false;  // one flag per instantiation
+    if (!big_smem) {
+        XG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(2 * BUF)));
+        big_smem = true;
+    }
+    const int res1 = resident_blocks(kern, k::ST_THREADS, BUF);
+    const int res2 = resident_blocks(kern, k::ST_THREADS, 2 * BUF);
+    const uint32_t nbuf = res2 >= res1 ? 2 : 1;
+    const int res = nbuf == 2 ? res2 : res1;
+    const uint64_t chunks = (A.st_S + TX - 1) / TX;
     const uint64_t groups = (A.nrows + (uint64_t)M * A.st_S - 1) / ((uint64_t)M * A.st_S);
-    const uint64_t threads = groups * A.st_S * (NV / VK);
-    const uint64_t blocks = (threads + k::ST_THREADS - 1) / k::ST_THREADS;
+    const uint64_t ntiles = groups * chunks;
+    const uint32_t P = (uint32_t)std::min<uint64_t>(ntiles, (uint64_t)res * ctx().sms);
     const k::StencilArgs a{A.st_val.p, A.st_mask.as<uint32_t>(), (uint32_t)A.nrows, A.st_S,
                            A.st_S2, A.st_diag_first ? 1 : 0};
-    if (A.st_pat == k::ST_BOX27)
-        k::k_spmv_stencil<F, F, NV, VK, M, k::ST_BOX27, Epi, V>
-            <<<(unsigned)blocks, k::ST_THREADS, 0, s>>>(a, x, epi);
-    else
-        k::k_spmv_stencil<F, F, NV, VK, M, k::ST_STAR7, Epi, V>
-            <<<(unsigned)blocks, k::ST_THREADS, 0, s>>>(a, x, epi);
+    kern<<<P, k::ST_THREADS, nbuf * BUF, s>>>(a, x, epi, nbuf, ctx().red().flag);
     XG_CUDA(cudaGetLastError());
     ++g_kernel_launches;
+}
+// regs: 0 the 64-register form, 1 the 128-register form
+template <typename F, int NV, typename V, class Epi>
+static void launch_stencil(const DCsr &A, const F *x, const Epi &epi, cudaStream_t s, int regs) {
+    if (A.st_pat == k::ST_BOX27) {
+        if (regs)
+            launch_stencil_p<F, NV, V, k::ST_BOX27, 4>(A, x, epi, s);
+        else
+            launch_stencil_p<F, NV, V, k::ST_BOX27, 8>(A, x, epi, s);
+    } else {
+        if (regs)
+            launch_stencil_p<F, NV, V, k::ST_STAR7, 4>(A, x, epi, s);
+        else
+            launch_stencil_p<F, NV, V, k::ST_STAR7, 8>(A, x, epi, s);
+    }
+}
+
+// Stencil or CSR (DCsr::st_choice): on matrices with a grid-stencil copy and
+// tuning on, the first SpMV without dot products for each precision and nv
+// times y = A x (EStore into a scratch y, the caller's x) with the stencil
+// kernel's two register budgets and with the CSR kernel's tuned shape (the
+// faster of two rounds of three launches each, outside any graph capture) and
+// keeps the fastest. All give the same results bit for bit.
+constexpr uint8_t ST_USE64 = 1, ST_USE128 = 2, ST_USE_CSR = 3;
+template <typename F, typename I, int NV, bool CALLER_X>
+static uint8_t tune_stencil(const DCsr &A, const F *x, cudaStream_t s) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    XG_CUDA(cudaStreamIsCapturing(s, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return 0;
+    DevBuf y(A.nrows * (uint64_t)NV * sizeof(F));
+    k::EStore<F, NV> e{{}, y.as<F>()};
+    cudaEvent_t e0, e1;
+    XG_CUDA(cudaEventCreate(&e0));
+    XG_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    uint8_t code = ST_USE64;
+    for (uint8_t c = ST_USE64; c <= ST_USE_CSR; ++c) {
+        auto go = [&] {
+            if (c == ST_USE_CSR) {
+                if constexpr (std::is_same<F, float>::value)
+                    if (A.bf16) {
+                        launch_v<F, F, I, NV, 0, CALLER_X, __nv_bfloat16>(A, x, e, s);
+                        return;
+                    }
+                launch_v<F, F, I, NV, 0, CALLER_X, F>(A, x, e, s);
+            } else if constexpr (std::is_same<F, float>::value) {
+                if (A.bf16)
+                    launch_stencil<F, NV, __nv_bfloat16>(A, x, e, s, c == ST_USE128);
+                else
+                    launch_stencil<F, NV, F>(A, x, e, s, c == ST_USE128);
+            } else {
+                launch_stencil<F, NV, F>(A, x, e, s, c == ST_USE128);
+            }
+        };
+        float ms = 1e30f;
+        go();  // untimed (tunes the CSR shape on its first call)
+        for (int round = 0; round < 2; ++round) {
+            XG_CUDA(cudaEventRecord(e0, s));
+            for (int r = 0; r < 3; ++r) go();
+            XG_CUDA(cudaEventRecord(e1, s));
+            XG_CUDA(cudaEventSynchronize(e1));
+            float t = 0;
+            XG_CUDA(cudaEventElapsedTime(&t, e0, e1));
+            ms = std::min(ms, t);
+        }
+        if (ms < best) {
+            best = ms;
+            code = c;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    XG_CUDA(cudaStreamSynchronize(s));
+    return code;
 }
 
 // FP32 matrices may store their values in BF16 (DCsr::bf16; gpu_level_bf16):
 // the kernel then widens each value to float as it reads it. SpMVs without
 // dot products on a matrix with a grid-stencil copy run the stencil kernel
-// (the same sums).
+// (the same sums) unless the autotuner measured the CSR kernel faster.
 template <typename F, typename FX, typename I, int NV, int NRED, bool CALLER_X = false,
           class Epi>
 static void launch(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s) {
@@ -295,13 +424,23 @@ static void launch(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s) {
     if constexpr (NRED == 0 && std::is_same<F, FX>::value) {
         constexpr uintptr_t SA = k::spmv_vk<F, NV>() * sizeof(F);
         if (A.st_pat >= 0 && (!CALLER_X || (uintptr_t)x % SA == 0)) {
-            if constexpr (std::is_same<F, float>::value)
-                if (A.bf16) {
-                    launch_stencil<F, NV, __nv_bfloat16>(A, x, epi, s);
-                    return;
-                }
-            launch_stencil<F, NV, F>(A, x, epi, s);
-            return;
+            int choice = A.st_force ? A.st_force : ST_USE64;
+            if (A.tune_on) {
+                int l = 0;
+                while ((1 << l) < NV) ++l;
+                uint8_t &c = A.st_choice[sizeof(F) == 4][l];
+                if (!c) c = tune_stencil<F, I, NV, CALLER_X>(A, x, s);
+                if (c) choice = c;
+            }
+            if (choice != ST_USE_CSR) {
+                if constexpr (std::is_same<F, float>::value)
+                    if (A.bf16) {
+                        launch_stencil<F, NV, __nv_bfloat16>(A, x, epi, s, choice == ST_USE128);
+                        return;
+                    }
+                launch_stencil<F, NV, F>(A, x, epi, s, choice == ST_USE128);
+                return;
+            }
         }
     }
     if constexpr (std::is_same<F, float>::value && std::is_same<FX, float>::value) {

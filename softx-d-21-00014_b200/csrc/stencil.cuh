@@ -12,7 +12,8 @@
 // The SpMV reads no column indices and no row pointers.
 //
 // Schedule: a thread carries M rows i, i+S, ..., i+(M-1)S (M consecutive grid
-// lines) and VK right-hand sides. For each plane dz and each of the M+2
+// lines) and VK right-hand sides; its values and masks come from shared
+// memory (staged below). For each plane dz and each of the M+2
 // lines l = -1..M around them it loads x at i + dz*S2 + l*S + dx once and adds
 // it to every carried row m it is a neighbour of (dy = l - m), so a
 // 27-point row costs 9(M+2)/M instead of 27 gathers of x; consecutive threads
@@ -56,76 +57,166 @@ struct StencilArgs {
 
 constexpr int ST_THREADS = 128;  // threads per block
 
-template <typename F, typename FX, int NV, int VK, int M, int PAT, class Epi, typename V = F>
-__global__ void __launch_bounds__(ST_THREADS, 8)
-    k_spmv_stencil(StencilArgs A, const FX *__restrict__ x, Epi epi) {
+// Tiles and staging. A tile is TX = ST_THREADS/G consecutive positions of a
+// group of M grid lines (rows b0 + m*S + p, p < TX); its K*M value runs and
+// M mask runs are copied into shared memory by the bulk-copy engine
+// (cp.async.bulk, completion on an mbarrier; unaligned run ends with plain
+// loads, as k_spmv stages its tiles), one or two buffers a block, the next
+// tile's copies issued before the current tile is computed. x is gathered
+// from global memory. Blocks are persistent (one wave) and take tiles
+// t = blockIdx.x, blockIdx.x + gridDim.x, ...
+__host__ __device__ constexpr uint32_t st_r16(uint32_t b) { return (b + 15u) & ~15u; }
+template <typename V, int G>
+__host__ __device__ constexpr uint32_t st_val_slot() {
+    return st_r16((ST_THREADS / G) * (uint32_t)sizeof(V) + 32u);
+}
+template <int G>
+__host__ __device__ constexpr uint32_t st_mask_slot() {
+    return st_r16((ST_THREADS / G) * 4u + 32u);
+}
+template <typename V, int G, int M, int PAT>
+__host__ __device__ constexpr uint32_t st_buffer_bytes() {
+    return (uint32_t)(st_slots<PAT>() * M) * st_val_slot<V, G>() + (uint32_t)M * st_mask_slot<G>();
+}
+
+// MINB: resident blocks the register budget is set for (8: 64 registers a
+// thread, 1,024 threads an SM, some spilled; 4: 128 registers, 512 threads,
+// more gathers in flight a thread); the autotuner picks between them.
+template <typename F, typename FX, int NV, int VK, int M, int PAT, int MINB, class Epi,
+          typename V = F>
+__global__ void __launch_bounds__(ST_THREADS, MINB)
+    k_spmv_stencil(StencilArgs A, const FX *__restrict__ x, Epi epi, uint32_t nbuf,
+                   unsigned *flag) {
     constexpr int G = NV / VK;
-    const uint32_t n = A.n, S = A.S;
-    const uint64_t t = (uint64_t)blockIdx.x * ST_THREADS + threadIdx.x;
-    const uint64_t slot_row = t / G;  // (group of M lines, position in the line)
-    const int k0 = (int)(t % G) * VK;
-    const uint64_t b = (slot_row / S) * (uint64_t)M * S + slot_row % S;
-    if (b >= n) return;
-    const V *__restrict__ val = (const V *)A.val;
-    uint32_t msk[M];
-    F y[M][VK];
-#pragma unroll
-    for (int m = 0; m < M; ++m) {
-        const uint64_t i = b + (uint64_t)m * S;
-        msk[m] = i < n ? __ldg(&A.mask[i]) : 0u;
-#pragma unroll
-        for (int v = 0; v < VK; ++v) y[m][v] = i < n ? epi.init(i, k0 + v) : F(0);
-    }
-    const int64_t bi = (int64_t)b;
-    const int64_t last = (int64_t)n - 1;
+    constexpr uint32_t TX = ST_THREADS / G;
+    constexpr int K = st_slots<PAT>();
+    constexpr int NRV = K * M, NR = NRV + M;  // staged runs: values (s, m), masks (m)
+    constexpr int NU = (NR + 31) / 32;        // runs a lane of warp 0 stages
+    constexpr uint32_t VS = st_val_slot<V, G>(), MS = st_mask_slot<G>();
+    constexpr uint32_t BUF = st_buffer_bytes<V, G, M, PAT>();
     constexpr int CENTER = st_slot<PAT>(0, 0, 0);
-    const bool df = A.diag_first != 0;
-    if (df) {
-#pragma unroll
-        for (int m = 0; m < M; ++m) {
-            const uint64_t i = b + (uint64_t)m * S;
-            const uint64_t ic = i < n ? i : (uint64_t)last;
-            FX xv[VK];
-            ld_x<FX, VK>(x + ((uint32_t)ic * (uint32_t)NV + (uint32_t)k0), xv);
-            const F av = val_as<F, V>(__ldg(&val[(uint64_t)CENTER * n + ic]));
-            const bool has = (msk[m] >> CENTER) & 1u;
-#pragma unroll
-            for (int v = 0; v < VK; ++v) {
-                const F sum = add(y[m][v], mul((F)xv[v], av));
-                y[m][v] = has ? sum : y[m][v];
-            }
-        }
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ uint8_t shift[2][NR];  // where run r's first row lands in its slot
+    const uint32_t n = A.n, S = A.S;
+    const V *__restrict__ val = (const V *)A.val;
+    const uint32_t *__restrict__ mask = A.mask;
+    const uint32_t nchunks = (S + TX - 1) / TX;
+    const uint32_t ngroups = (uint32_t)(((uint64_t)n + (uint64_t)M * S - 1) / ((uint64_t)M * S));
+    const uint32_t ntiles = ngroups * nchunks;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t p = threadIdx.x / G;
+    const int k0 = (threadIdx.x % G) * VK;
+    if (threadIdx.x == 0) {
+        mbar_init(&mbar[0], 1);
+        mbar_init(&mbar[1], 1);
+        mbar_init_fence();
     }
+    __syncthreads();
+    uint32_t n_issued = 0, n_used = 0;
+    bool timed_out = false;
+    // warp 0: stage tile t (rows b0 + m*S + [0, w) of each line m, cut at n)
+    // into the next buffer
+    auto issue = [&](uint32_t t) {
+        if (t >= ntiles) return;
+        const uint32_t bsel = n_issued % nbuf;
+        unsigned char *buf = smem_raw + (size_t)bsel * BUF;
+        uint64_t *mb = &mbar[bsel];
+        ++n_issued;
+        const uint32_t x0 = (t % nchunks) * TX;
+        const uint32_t b0 = (t / nchunks) * (uint32_t)M * S + x0;
+        const uint32_t w = S - x0 < TX ? S - x0 : TX;
+        const void *src[NU];
+        void *dst[NU];
+        uint32_t nb[NU];
+        uint32_t total = 0;
 #pragma unroll
-    for (int dz = -1; dz <= 1; ++dz) {
-#pragma unroll
-        for (int l = -1; l <= M; ++l) {
-#pragma unroll
-            for (int dx = -1; dx <= 1; ++dx) {
-                // the carried rows this x row is a neighbour of (compile time)
-                bool any = false;
-#pragma unroll
-                for (int m = 0; m < M; ++m) {
-                    const int dy = l - m;
-                    if (dy >= -1 && dy <= 1 && st_slot<PAT>(dz, dy, dx) >= 0) any = true;
+        for (int u = 0; u < NU; ++u) {
+            const int r = lane + 32 * u;
+            nb[u] = 0;
+            if (r < NR) {
+                const int m = r < NRV ? r % M : r - NRV;
+                const uint64_t rb = (uint64_t)b0 + (uint64_t)m * S;
+                const uint32_t r0 = rb < n ? (uint32_t)rb : n;
+                const uint32_t r1 = rb + w < n ? (uint32_t)(rb + w) : n;
+                if (r < NRV) {
+                    const uint32_t e0 = (uint32_t)(r / M) * n + r0;
+                    shift[bsel][r] = (uint8_t)stage_shift<V>(val, e0);
+                    if (r1 > r0) {
+                        const V *sp;
+                        V *dp;
+                        nb[u] = stage_range<V>((V *)(buf + (size_t)r * VS), val,
+                                               (uint64_t)K * n, e0, e0 + (r1 - r0), sp, dp);
+                        src[u] = sp;
+                        dst[u] = dp;
+                    }
+                } else {
+                    shift[bsel][r] = (uint8_t)stage_shift<uint32_t>(mask, r0);
+                    if (r1 > r0) {
+                        const uint32_t *sp;
+                        uint32_t *dp;
+                        nb[u] = stage_range<uint32_t>(
+                            (uint32_t *)(buf + (size_t)NRV * VS + (size_t)m * MS), mask, n, r0,
+                            r1, sp, dp);
+                        src[u] = sp;
+                        dst[u] = dp;
+                    }
                 }
-                if (!any) continue;
-                int64_t c = bi + (int64_t)dz * A.S2 + (int64_t)l * S + dx;
-                // rows that have none of these entries may point outside x:
-                // read a valid row instead (its values are not used)
-                c = c < 0 ? 0 : (c > last ? last : c);
-                FX xv[VK];
-                ld_x<FX, VK>(x + ((uint32_t)c * (uint32_t)NV + (uint32_t)k0), xv);
+            }
+            total += nb[u];
+        }
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) total += __shfl_xor_sync(0xffffffffu, total, off);
+        __syncwarp();
+        if (lane == 0) mbar_arrive_expect(mb, total);  // releases the plain-load writes
+        __syncwarp();
+        fence_proxy_async_smem();
+#pragma unroll
+        for (int u = 0; u < NU; ++u)
+            if (nb[u]) bulk_g2s(dst[u], src[u], nb[u], mb);
+    };
+    if (warp == 0) issue(blockIdx.x);
+    const int64_t last = (int64_t)n - 1;
+    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const uint32_t tn = t + gridDim.x;
+        if (nbuf == 2 && warp == 0) issue(tn);
+        const uint32_t bsel = n_used % nbuf;
+        // a copy that never landed: every thread of the block stops here
+        if (__syncthreads_or(!mbar_wait(&mbar[bsel], (n_used / nbuf) & 1u))) {
+            timed_out = true;
+            break;
+        }
+        ++n_used;
+        const unsigned char *buf = smem_raw + (size_t)bsel * BUF;
+        const uint32_t x0 = (t % nchunks) * TX;
+        const uint32_t i0 = (t / nchunks) * (uint32_t)M * S + x0 + p;  // row of line 0
+        const uint32_t w = S - x0 < TX ? S - x0 : TX;
+        if (p < w && i0 < n) {
+            // staged value of slot s for line m's row
+            auto vat = [&](int s, int m) -> V {
+                const int r = s * M + m;
+                return ((const V *)(buf + (size_t)r * VS))[shift[bsel][r] + p];
+            };
+            uint32_t msk[M];
+            F y[M][VK];
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+                const uint64_t i = (uint64_t)i0 + (uint64_t)m * S;
+                const bool in = i < n;
+                const uint32_t *mr = (const uint32_t *)(buf + (size_t)NRV * VS + (size_t)m * MS);
+                msk[m] = in ? mr[shift[bsel][NRV + m] + p] : 0u;
+#pragma unroll
+                for (int v = 0; v < VK; ++v) y[m][v] = in ? epi.init(i, k0 + v) : F(0);
+            }
+            const bool df = A.diag_first != 0;
+            if (df) {
 #pragma unroll
                 for (int m = 0; m < M; ++m) {
-                    const int dy = l - m;
-                    if (dy < -1 || dy > 1) continue;
-                    const int s = st_slot<PAT>(dz, dy, dx);
-                    if (s < 0) continue;
-                    const uint64_t i = b + (uint64_t)m * S;
-                    const uint64_t ic = i < n ? i : (uint64_t)last;
-                    const F av = val_as<F, V>(__ldg(&val[(uint64_t)s * n + ic]));
-                    const bool has = ((msk[m] >> s) & 1u) && !(s == CENTER && df);
+                    const bool has = (msk[m] >> CENTER) & 1u;
+                    const uint32_t ic = has ? i0 + (uint32_t)m * S : 0u;
+                    FX xv[VK];
+                    ld_x<FX, VK>(x + (ic * (uint32_t)NV + (uint32_t)k0), xv);
+                    const F av = val_as<F, V>(vat(CENTER, m));
 #pragma unroll
                     for (int v = 0; v < VK; ++v) {
                         const F sum = add(y[m][v], mul((F)xv[v], av));
@@ -133,16 +224,61 @@ __global__ void __launch_bounds__(ST_THREADS, 8)
                     }
                 }
             }
+#pragma unroll
+            for (int dz = -1; dz <= 1; ++dz) {
+#pragma unroll
+                for (int l = -1; l <= M; ++l) {
+#pragma unroll
+                    for (int dx = -1; dx <= 1; ++dx) {
+                        // the carried rows this x row is a neighbour of (compile time)
+                        bool any = false;
+#pragma unroll
+                        for (int m = 0; m < M; ++m) {
+                            const int dy = l - m;
+                            if (dy >= -1 && dy <= 1 && st_slot<PAT>(dz, dy, dx) >= 0) any = true;
+                        }
+                        if (!any) continue;
+                        int64_t c = (int64_t)i0 + (int64_t)dz * A.S2 + (int64_t)l * S + dx;
+                        // rows that have none of these entries may point outside x:
+                        // read a valid row instead (its values are not used)
+                        c = c < 0 ? 0 : (c > last ? last : c);
+                        FX xv[VK];
+                        ld_x<FX, VK>(x + ((uint32_t)c * (uint32_t)NV + (uint32_t)k0), xv);
+#pragma unroll
+                        for (int m = 0; m < M; ++m) {
+                            const int dy = l - m;
+                            if (dy < -1 || dy > 1) continue;
+                            const int s = st_slot<PAT>(dz, dy, dx);
+                            if (s < 0) continue;
+                            const bool has = ((msk[m] >> s) & 1u) && !(s == CENTER && df);
+                            const F av = val_as<F, V>(vat(s, m));
+#pragma unroll
+                            for (int v = 0; v < VK; ++v) {
+                                const F sum = add(y[m][v], mul((F)xv[v], av));
+                                y[m][v] = has ? sum : y[m][v];
+                            }
+                        }
+                    }
+                }
+            }
+            F none[1] = {F(0)};
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+                const uint64_t i = (uint64_t)i0 + (uint64_t)m * S;
+                if (i < n) {
+#pragma unroll
+                    for (int v = 0; v < VK; ++v) epi.store(i, k0 + v, y[m][v], none);
+                }
+            }
         }
+        __syncthreads();  // every reader is done with this tile's buffer
+        if (nbuf == 1 && warp == 0) issue(tn);
     }
-    F none[1] = {F(0)};
-#pragma unroll
-    for (int m = 0; m < M; ++m) {
-        const uint64_t i = b + (uint64_t)m * S;
-        if (i < n) {
-#pragma unroll
-            for (int v = 0; v < VK; ++v) epi.store(i, k0 + v, y[m][v], none);
-        }
+    if (timed_out && threadIdx.x == 0) {
+        // raise the flag; no block exits with a copy into its shared memory
+        // still in flight (bounded waits)
+        atomicOr(flag, 1u);
+        for (uint32_t u = n_used; u < n_issued; ++u) mbar_wait(&mbar[u % nbuf], (u / nbuf) & 1u);
     }
 }
 

@@ -152,3 +152,29 @@ def test_bf16_cycle_operators_bit_exact(gpu, oracle, nv, tune):
     r1, c1, v1, info = S.level_download(1, 3)
     x1, y01, y1, ya1 = run_level_spmv(gpu, S, 1, 3, r1, c1, v1, nv, True, seed=nv + 1)
     assert y1.tobytes() == oracle.csr_ax_y(r1, c1.astype(np.uint32), v1, x1, nv).tobytes()
+
+
+@pytest.mark.parametrize("nv", [1, 2, 8, 32])
+@pytest.mark.parametrize("f32", [False, True])
+def test_warp_per_row_kernel_bit_exact(gpu, oracle, nv, f32):
+    """The warp-per-row SpMV (gpu_spmv_tune = 3; an autotuner candidate for
+    small matrices) on rows long enough to span several chunks of its
+    shared-memory product buffer: every element equals the oracle's
+    sequential row sum, for y = A x and y += A x."""
+    row, col, val = banded_plus_random(1500, 700, 300, seed=nv + 50)
+    krylov = {"method": "MergedPBiCGStab", "rel_tolerance": 1e-8, "max_iters": 5,
+              "gpu_spmv_tune": 3}
+    params = {"solver": krylov}
+    if f32:
+        params = {"solver": dict(krylov, gpu_index_compress=2),
+                  "preconditioner": {"method": "MultiGrid", "mg_max_levels": 2,
+                                     "mg_coarsening_type": 8, "mg_interpolation_type": 6,
+                                     "mg_agg_num_levels": 0, "gpu_precond_f32": 1,
+                                     "gpu_spmv_tune": 3},
+                  "pre_smoother": {"method": "Jacobi"}, "post_smoother": {"method": "Jacobi"}}
+    _, _, _, S = solver_on(gpu, row, col, val, nv, params)
+    which = 3 if f32 else 0
+    xh, y0, y, ya = run_level_spmv(gpu, S, 0, which, row, col, val, nv, f32, seed=nv)
+    v = val.astype(np.float32) if f32 else val
+    assert y.tobytes() == oracle.csr_ax_y(row, col, v, xh, nv).tobytes()
+    assert ya.tobytes() == oracle.csr_ax_y(row, col, v, xh, nv, axpy_y=y0).tobytes()

@@ -30,12 +30,16 @@ MATS = {
 }
 
 
-def params(compress, f32, bf16, smoother="Chebyshev"):
+def params(compress, f32, bf16, smoother="Chebyshev", tune=0):
+    """tune: gpu_spmv_tune (0: the stencil kernel's 64-register form, 2: its
+    128-register form, 1: whichever of those and the CSR kernel measured
+    fastest)."""
     prec = {"method": "MultiGrid", "mg_max_levels": 3, "mg_coarsening_type": 8,
             "mg_interpolation_type": 6, "mg_agg_num_levels": 0, "gpu_index_compress": compress,
-            "gpu_precond_f32": 1 if f32 else 0, "gpu_level_bf16": 1 if bf16 else 0}
+            "gpu_precond_f32": 1 if f32 else 0, "gpu_level_bf16": 1 if bf16 else 0,
+            "gpu_spmv_tune": tune}
     return {"solver": {"method": "MergedPBiCGStab", "rel_tolerance": 1e-8, "max_iters": 100,
-                       "abs_tolerance": 0, "gpu_index_compress": compress},
+                       "abs_tolerance": 0, "gpu_index_compress": compress, "gpu_spmv_tune": tune},
             "preconditioner": prec, "pre_smoother": {"method": smoother},
             "post_smoother": {"method": smoother}, "coarse_grid_solver": {"method": "Direct"}}
 
@@ -66,12 +70,13 @@ def level0_spmv(S, nv, f32, seed):
 @pytest.mark.parametrize("mat", list(MATS))
 @pytest.mark.parametrize("form", ["f64", "f32", "bf16"])
 @pytest.mark.parametrize("nv", [1, 2, 4, 8, 16, 32])
-def test_level0_spmv_same_bits(gpu, oracle, mat, form, nv):
+@pytest.mark.parametrize("tune", [0, 2])
+def test_level0_spmv_same_bits(gpu, oracle, mat, form, nv, tune):
     row, col, val = MATS[mat](gpu)
     f32, bf16 = form != "f64", form == "bf16"
     out = {}
     for compress in (2, 3):
-        _, _, _, S = build(gpu, row, col, val, nv, params(compress, f32, bf16))
+        _, _, _, S = build(gpu, row, col, val, nv, params(compress, f32, bf16, tune=tune))
         pat = S.level_stencil(0, 3)
         if compress == 3:
             assert pat[0] == (0 if mat.startswith("fe27") else 1), pat
@@ -90,8 +95,11 @@ def test_level0_spmv_same_bits(gpu, oracle, mat, form, nv):
 @pytest.mark.parametrize("mat", list(MATS))
 @pytest.mark.parametrize("form,smoother", [("f64", "Chebyshev"), ("f32", "Chebyshev"),
                                            ("bf16", "Chebyshev"), ("f32", "Jacobi")])
-def test_solves_same_bits(gpu, mat, form, smoother):
-    """Whole preconditioned solves: same iterations and solution bits."""
+@pytest.mark.parametrize("tune", [0, 1])
+def test_solves_same_bits(gpu, mat, form, smoother, tune):
+    """Whole preconditioned solves: same iterations and solution bits (with
+    the autotuner on, the stencil and CSR kernels give the same bits
+    whichever it picks)."""
     row, col, val = MATS[mat](gpu)
     nv = 4
     n = len(row) - 1
@@ -99,7 +107,7 @@ def test_solves_same_bits(gpu, mat, form, smoother):
     res = {}
     for compress in (2, 3):
         _, xv, bv, S = build(gpu, row, col, val, nv,
-                             params(compress, form != "f64", form == "bf16", smoother))
+                             params(compress, form != "f64", form == "bf16", smoother, tune))
         bv.upload(b)
         for _ in range(2):  # the second solve replays the recorded graphs
             xv.set(0.0)
