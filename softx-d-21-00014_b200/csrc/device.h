@@ -146,10 +146,12 @@ struct DCsr {
     mutable uint8_t tuned[2][2][6] = {};
     // Grid-stencil copy (gpu_index_compress = 3, csrc/stencil.cuh): the slot
     // pattern (-1: none, else k::ST_BOX27 or k::ST_STAR7), the line and plane
-    // strides, the row order, the [slots][nrows] values in the CSR values'
-    // type and the per-row entry masks. The SpMVs without dot products use it.
+    // strides, the row order, the per-slot values in the CSR values' type and
+    // the per-row entry masks (lines padded, csrc/stencil.cuh). The SpMVs
+    // without dot products use it.
     int st_pat = -1;
-    uint32_t st_S = 0, st_S2 = 0;
+    uint32_t st_S = 0, st_S2 = 0, st_SP = 0;  // strides; padded line length
+    uint64_t st_slot = 0;                     // elements per slot array
     bool st_diag_first = false;  // rows store their diagonal first
     DevBuf st_val, st_mask;
     // with tuning on: the kernel measured fastest for the SpMVs without dot

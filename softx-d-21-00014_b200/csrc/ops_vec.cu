@@ -353,15 +353,23 @@ static void upload_stencil(const HCsr &h, DCsr &d, cudaStream_t s) {
     if (!stencil_layout(h, pat, S, S2, df)) return;
     const uint64_t n = h.nrows;
     const int K = pat == k::ST_BOX27 ? k::st_slots<k::ST_BOX27>() : k::st_slots<k::ST_STAR7>();
-    std::vector<uint32_t> mask(n, 0u);
-    std::vector<double> v((size_t)K * n, 0.0);
+    // padded layout (csrc/stencil.cuh): row i at line (i / S) * SP + i % S of
+    // its slot's array, lines padded to whole groups, one tile of slack
+    const uint64_t SP = (S + k::ST_LINE_PAD - 1) / k::ST_LINE_PAD * k::ST_LINE_PAD;
+    const uint64_t M = k::ST_LINES;
+    const uint64_t LP = (n + M * S - 1) / (M * S) * M;
+    const uint64_t slot_len = LP * SP, pad = k::ST_THREADS;
+    std::vector<uint32_t> mask(slot_len + pad, 0u);
+    std::vector<double> v((size_t)K * slot_len + pad, 0.0);
     SlotCache slot{pat, S, S2, {}};
-    for (uint64_t i = 0; i < n; ++i)
+    for (uint64_t i = 0; i < n; ++i) {
+        const uint64_t at = (i / S) * SP + i % S;
         for (uint64_t j = h.row[i]; j < h.row[i + 1]; ++j) {
             const int sl = slot((int64_t)h.col[j] - (int64_t)i);
-            mask[i] |= 1u << sl;
-            v[(size_t)sl * n + i] = h.val[j];
+            mask[at] |= 1u << sl;
+            v[(size_t)sl * slot_len + at] = h.val[j];
         }
+    }
     upload(d.st_mask, mask, s);
     if (d.bf16) {
         std::vector<__nv_bfloat16> w(v.size());
@@ -380,6 +388,8 @@ static void upload_stencil(const HCsr &h, DCsr &d, cudaStream_t s) {
     d.st_pat = pat;
     d.st_S = S;
     d.st_S2 = S2;
+    d.st_SP = (uint32_t)SP;
+    d.st_slot = slot_len;
     d.st_diag_first = df;
 }
 

@@ -306,34 +306,37 @@ static void launch_v(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s)
 // The grid-stencil kernel (csrc/stencil.cuh) on a matrix's stencil copy: M
 // grid lines a thread, as many right-hand sides a thread as the CSR kernel
 // carries; one wave of persistent blocks over the tiles, two staging buffers
-// a block unless that lowers the resident blocks.
-constexpr int ST_LINES = 4;
+// a block unless that lowers the resident blocks or does not fit.
 template <typename F, int NV, typename V, int PAT, int MINB, class Epi>
 static void launch_stencil_p(const DCsr &A, const F *x, const Epi &epi, cudaStream_t s) {
     constexpr int VK = k::spmv_vk<F, NV>();
     constexpr int G = NV / VK;
-    constexpr int M = ST_LINES;
-    constexpr uint32_t TX = k::ST_THREADS / G;
+    constexpr int M = k::ST_LINES;
+    constexpr uint32_t TX = k::st_tx<G>();
     constexpr uint32_t BUF = k::st_buffer_bytes<V, G, M, PAT>();
+    constexpr uint32_t SMEM_MAX = 227u * 1024u;
+    static_assert(BUF <= SMEM_MAX, "stencil staging buffer exceeds shared memory");
+    constexpr bool TWO = 2 * BUF <= SMEM_MAX;
     XG_REQUIRE(A.nrows * (uint64_t)NV < (1ull << 32), XAMG_ERR_UNSUPPORTED,
                "SpMV: x of 2^32 or more values");
     auto kern = k::k_spmv_stencil<F, F, NV, VK, M, PAT, MINB, Epi, V>;
     static bool big_smem = false;  // one flag per instantiation
     if (!big_smem) {
         XG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(2 * BUF)));
+                                     (int)(TWO ? 2 * BUF : BUF)));
         big_smem = true;
     }
     const int res1 = resident_blocks(kern, k::ST_THREADS, BUF);
-    const int res2 = resident_blocks(kern, k::ST_THREADS, 2 * BUF);
+    const int res2 = TWO ? resident_blocks(kern, k::ST_THREADS, 2 * BUF) : 0;
     const uint32_t nbuf = res2 >= res1 ? 2 : 1;
     const int res = nbuf == 2 ? res2 : res1;
     const uint64_t chunks = (A.st_S + TX - 1) / TX;
     const uint64_t groups = (A.nrows + (uint64_t)M * A.st_S - 1) / ((uint64_t)M * A.st_S);
     const uint64_t ntiles = groups * chunks;
     const uint32_t P = (uint32_t)std::min<uint64_t>(ntiles, (uint64_t)res * ctx().sms);
-    const k::StencilArgs a{A.st_val.p, A.st_mask.as<uint32_t>(), (uint32_t)A.nrows, A.st_S,
-                           A.st_S2, A.st_diag_first ? 1 : 0};
+    const k::StencilArgs a{A.st_val.p,  A.st_mask.as<uint32_t>(), (uint32_t)A.nrows, A.st_S,
+                           A.st_S2,     A.st_SP,                  A.st_slot,
+                           A.st_diag_first ? 1 : 0};
     kern<<<P, k::ST_THREADS, nbuf * BUF, s>>>(a, x, epi, nbuf, ctx().red().flag);
     XG_CUDA(cudaGetLastError());
     ++g_kernel_launches;

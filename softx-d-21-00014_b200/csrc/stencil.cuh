@@ -6,9 +6,10 @@
 // finest level of a structured-grid problem) needs no column indices: the
 // offset of each of its K slots is known. The upload keeps the CSR block and
 // adds a copy in this form (gpu_index_compress = 3):
-//   val[s][i]: the value of row i's entry in slot s (slot order = ascending
-//              offset), 0 where row i has no such entry;
-//   mask[i]:   bit s set where row i has the entry of slot s.
+//   val[s][.]: the value of each row's entry in slot s (slot order =
+//              ascending offset), 0 where the row has no such entry;
+//   mask[.]:   bit s set where the row has the entry of slot s
+// (rows at padded positions, below).
 // The SpMV reads no column indices and no row pointers.
 //
 // Schedule: a thread carries M rows i, i+S, ..., i+(M-1)S (M consecutive grid
@@ -49,56 +50,71 @@ __host__ __device__ constexpr int st_slot(int dz, int dy, int dx) {
 }
 
 struct StencilArgs {
-    const void *val;       // [K][n] values (stored type V)
-    const uint32_t *mask;  // [n]
+    const void *val;       // [K][LP][SP] values (stored type V)
+    const uint32_t *mask;  // [LP][SP]
     uint32_t n, S, S2;
+    uint32_t SP;           // padded line length (a multiple of 8)
+    uint64_t slot;         // elements per slot array: LP * SP
     int diag_first;        // rows store their diagonal first
 };
 
 constexpr int ST_THREADS = 128;  // threads per block
+constexpr int ST_LINES = 4;      // grid lines a thread carries (M)
+constexpr uint32_t ST_LINE_PAD = 8;
 
-// Tiles and staging. A tile is TX = ST_THREADS/G consecutive positions of a
-// group of M grid lines (rows b0 + m*S + p, p < TX); its K*M value runs and
-// M mask runs are copied into shared memory by the bulk-copy engine
-// (cp.async.bulk, completion on an mbarrier; unaligned run ends with plain
-// loads, as k_spmv stages its tiles), one or two buffers a block, the next
-// tile's copies issued before the current tile is computed. x is gathered
-// from global memory. Blocks are persistent (one wave) and take tiles
-// t = blockIdx.x, blockIdx.x + gridDim.x, ...
-__host__ __device__ constexpr uint32_t st_r16(uint32_t b) { return (b + 15u) & ~15u; }
-template <typename V, int G>
-__host__ __device__ constexpr uint32_t st_val_slot() {
-    return st_r16((ST_THREADS / G) * (uint32_t)sizeof(V) + 32u);
-}
+// Stored layout: row i = line L * S + x is kept at element L * SP + x of its
+// slot's array (SP = S rounded up to a multiple of 8), lines padded to a
+// multiple of ST_LINES (and the arrays by one tile), so that every run a
+// tile stages starts 16-byte aligned and has a fixed length.
+//
+// Tiles and staging. A tile is TX = ST_THREADS/G consecutive positions x0 ..
+// x0+TX-1 of a group of M grid lines; its K*M value runs and M mask runs
+// (TX elements each, those past the line unused) are copied into shared
+// memory by the bulk-copy engine (cp.async.bulk, completion on an
+// mbarrier), one or two buffers a block, the next tile's copies issued
+// before the current tile is computed. x is gathered from global memory.
+// Blocks are persistent (one wave) and take tiles t = blockIdx.x,
+// blockIdx.x + gridDim.x, ...
 template <int G>
-__host__ __device__ constexpr uint32_t st_mask_slot() {
-    return st_r16((ST_THREADS / G) * 4u + 32u);
-}
+__host__ __device__ constexpr uint32_t st_tx() { return ST_THREADS / G; }
 template <typename V, int G, int M, int PAT>
 __host__ __device__ constexpr uint32_t st_buffer_bytes() {
-    return (uint32_t)(st_slots<PAT>() * M) * st_val_slot<V, G>() + (uint32_t)M * st_mask_slot<G>();
+    return (uint32_t)(st_slots<PAT>() * M) * st_tx<G>() * (uint32_t)sizeof(V) +
+           (uint32_t)M * st_tx<G>() * 4u;
+}
+
+// y[m][v] += x * a for the entries each carried row has (has: the select
+// that skips an absent entry; FAST: every carried row has every entry of the
+// pattern, so no select is needed).
+template <typename F, int VK>
+__device__ __forceinline__ void st_acc(F (&y)[VK], const F (&xv)[VK], F av, bool has) {
+#pragma unroll
+    for (int v = 0; v < VK; ++v) {
+        const F sum = add(y[v], mul(xv[v], av));
+        y[v] = has ? sum : y[v];
+    }
 }
 
 // MINB: resident blocks the register budget is set for (8: 64 registers a
-// thread, 1,024 threads an SM, some spilled; 4: 128 registers, 512 threads,
-// more gathers in flight a thread); the autotuner picks between them.
+// thread, 1,024 threads an SM; 4: 128 registers, 512 threads, more gathers in
+// flight a thread); the autotuner picks between them.
 template <typename F, typename FX, int NV, int VK, int M, int PAT, int MINB, class Epi,
           typename V = F>
 __global__ void __launch_bounds__(ST_THREADS, MINB)
     k_spmv_stencil(StencilArgs A, const FX *__restrict__ x, Epi epi, uint32_t nbuf,
                    unsigned *flag) {
     constexpr int G = NV / VK;
-    constexpr uint32_t TX = ST_THREADS / G;
+    constexpr uint32_t TX = st_tx<G>();
     constexpr int K = st_slots<PAT>();
     constexpr int NRV = K * M, NR = NRV + M;  // staged runs: values (s, m), masks (m)
     constexpr int NU = (NR + 31) / 32;        // runs a lane of warp 0 stages
-    constexpr uint32_t VS = st_val_slot<V, G>(), MS = st_mask_slot<G>();
     constexpr uint32_t BUF = st_buffer_bytes<V, G, M, PAT>();
+    constexpr uint32_t VRUN = TX * (uint32_t)sizeof(V);
     constexpr int CENTER = st_slot<PAT>(0, 0, 0);
+    constexpr uint32_t FULL = PAT == ST_BOX27 ? 0x7ffffffu : 0x7fu;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t mbar[2];
-    __shared__ uint8_t shift[2][NR];  // where run r's first row lands in its slot
-    const uint32_t n = A.n, S = A.S;
+    const uint32_t n = A.n, S = A.S, SP = A.SP;
     const V *__restrict__ val = (const V *)A.val;
     const uint32_t *__restrict__ mask = A.mask;
     const uint32_t nchunks = (S + TX - 1) / TX;
@@ -115,68 +131,33 @@ __global__ void __launch_bounds__(ST_THREADS, MINB)
     __syncthreads();
     uint32_t n_issued = 0, n_used = 0;
     bool timed_out = false;
-    // warp 0: stage tile t (rows b0 + m*S + [0, w) of each line m, cut at n)
-    // into the next buffer
+    // warp 0: stage tile t into the next buffer
     auto issue = [&](uint32_t t) {
         if (t >= ntiles) return;
         const uint32_t bsel = n_issued % nbuf;
         unsigned char *buf = smem_raw + (size_t)bsel * BUF;
         uint64_t *mb = &mbar[bsel];
         ++n_issued;
-        const uint32_t x0 = (t % nchunks) * TX;
-        const uint32_t b0 = (t / nchunks) * (uint32_t)M * S + x0;
-        const uint32_t w = S - x0 < TX ? S - x0 : TX;
-        const void *src[NU];
-        void *dst[NU];
-        uint32_t nb[NU];
-        uint32_t total = 0;
-#pragma unroll
-        for (int u = 0; u < NU; ++u) {
-            const int r = lane + 32 * u;
-            nb[u] = 0;
-            if (r < NR) {
-                const int m = r < NRV ? r % M : r - NRV;
-                const uint64_t rb = (uint64_t)b0 + (uint64_t)m * S;
-                const uint32_t r0 = rb < n ? (uint32_t)rb : n;
-                const uint32_t r1 = rb + w < n ? (uint32_t)(rb + w) : n;
-                if (r < NRV) {
-                    const uint32_t e0 = (uint32_t)(r / M) * n + r0;
-                    shift[bsel][r] = (uint8_t)stage_shift<V>(val, e0);
-                    if (r1 > r0) {
-                        const V *sp;
-                        V *dp;
-                        nb[u] = stage_range<V>((V *)(buf + (size_t)r * VS), val,
-                                               (uint64_t)K * n, e0, e0 + (r1 - r0), sp, dp);
-                        src[u] = sp;
-                        dst[u] = dp;
-                    }
-                } else {
-                    shift[bsel][r] = (uint8_t)stage_shift<uint32_t>(mask, r0);
-                    if (r1 > r0) {
-                        const uint32_t *sp;
-                        uint32_t *dp;
-                        nb[u] = stage_range<uint32_t>(
-                            (uint32_t *)(buf + (size_t)NRV * VS + (size_t)m * MS), mask, n, r0,
-                            r1, sp, dp);
-                        src[u] = sp;
-                        dst[u] = dp;
-                    }
-                }
-            }
-            total += nb[u];
-        }
-#pragma unroll
-        for (int off = 16; off >= 1; off >>= 1) total += __shfl_xor_sync(0xffffffffu, total, off);
-        __syncwarp();
-        if (lane == 0) mbar_arrive_expect(mb, total);  // releases the plain-load writes
+        const uint64_t line0 = (uint64_t)(t / nchunks) * M, x0 = (t % nchunks) * TX;
+        if (lane == 0) mbar_arrive_expect(mb, BUF);
         __syncwarp();
         fence_proxy_async_smem();
 #pragma unroll
-        for (int u = 0; u < NU; ++u)
-            if (nb[u]) bulk_g2s(dst[u], src[u], nb[u], mb);
+        for (int u = 0; u < NU; ++u) {
+            const int r = lane + 32 * u;
+            if (r < NRV) {
+                const uint64_t e = (uint64_t)(r / M) * A.slot + (line0 + r % M) * SP + x0;
+                bulk_g2s(buf + (size_t)r * VRUN, val + e, VRUN, mb);
+            } else if (r < NR) {
+                const uint64_t e = (line0 + (r - NRV)) * SP + x0;
+                bulk_g2s(buf + (size_t)NRV * VRUN + (size_t)(r - NRV) * TX * 4u, mask + e, TX * 4u,
+                         mb);
+            }
+        }
     };
     if (warp == 0) issue(blockIdx.x);
     const int64_t last = (int64_t)n - 1;
+    const bool df = A.diag_first != 0;
     for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const uint32_t tn = t + gridDim.x;
         if (nbuf == 2 && warp == 0) issue(tn);
@@ -188,79 +169,91 @@ __global__ void __launch_bounds__(ST_THREADS, MINB)
         }
         ++n_used;
         const unsigned char *buf = smem_raw + (size_t)bsel * BUF;
+        const V *vb = (const V *)buf + p;  // value of slot s, line m: vb[(s * M + m) * TX]
+        const uint32_t *mbuf = (const uint32_t *)(buf + (size_t)NRV * VRUN) + p;
         const uint32_t x0 = (t % nchunks) * TX;
         const uint32_t i0 = (t / nchunks) * (uint32_t)M * S + x0 + p;  // row of line 0
-        const uint32_t w = S - x0 < TX ? S - x0 : TX;
-        if (p < w && i0 < n) {
-            // staged value of slot s for line m's row
-            auto vat = [&](int s, int m) -> V {
-                const int r = s * M + m;
-                return ((const V *)(buf + (size_t)r * VS))[shift[bsel][r] + p];
-            };
-            uint32_t msk[M];
+        const bool active = x0 + p < S && i0 < n;
+        uint32_t msk[M];
+        bool full = active;
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+            msk[m] = active && (uint64_t)i0 + (uint64_t)m * S < n ? mbuf[m * TX] : 0u;
+            full = full && msk[m] == FULL;
+        }
+        // a warp whose rows all have the whole pattern takes the path
+        // without selects and clamps
+        const bool fast = __all_sync(0xffffffffu, full);
+        if (active) {
             F y[M][VK];
 #pragma unroll
             for (int m = 0; m < M; ++m) {
                 const uint64_t i = (uint64_t)i0 + (uint64_t)m * S;
-                const bool in = i < n;
-                const uint32_t *mr = (const uint32_t *)(buf + (size_t)NRV * VS + (size_t)m * MS);
-                msk[m] = in ? mr[shift[bsel][NRV + m] + p] : 0u;
 #pragma unroll
-                for (int v = 0; v < VK; ++v) y[m][v] = in ? epi.init(i, k0 + v) : F(0);
+                for (int v = 0; v < VK; ++v) y[m][v] = i < n ? epi.init(i, k0 + v) : F(0);
             }
-            const bool df = A.diag_first != 0;
             if (df) {
 #pragma unroll
                 for (int m = 0; m < M; ++m) {
                     const bool has = (msk[m] >> CENTER) & 1u;
                     const uint32_t ic = has ? i0 + (uint32_t)m * S : 0u;
-                    FX xv[VK];
-                    ld_x<FX, VK>(x + (ic * (uint32_t)NV + (uint32_t)k0), xv);
-                    const F av = val_as<F, V>(vat(CENTER, m));
+                    FX xr[VK];
+                    ld_x<FX, VK>(x + (ic * (uint32_t)NV + (uint32_t)k0), xr);
+                    F xv[VK];
 #pragma unroll
-                    for (int v = 0; v < VK; ++v) {
-                        const F sum = add(y[m][v], mul((F)xv[v], av));
-                        y[m][v] = has ? sum : y[m][v];
-                    }
+                    for (int v = 0; v < VK; ++v) xv[v] = (F)xr[v];
+                    st_acc<F, VK>(y[m], xv, val_as<F, V>(vb[(CENTER * M + m) * TX]), has);
                 }
             }
+            auto body = [&](auto fastc) {
+                constexpr bool FAST = decltype(fastc)::value;
 #pragma unroll
-            for (int dz = -1; dz <= 1; ++dz) {
+                for (int dz = -1; dz <= 1; ++dz) {
 #pragma unroll
-                for (int l = -1; l <= M; ++l) {
+                    for (int l = -1; l <= M; ++l) {
 #pragma unroll
-                    for (int dx = -1; dx <= 1; ++dx) {
-                        // the carried rows this x row is a neighbour of (compile time)
-                        bool any = false;
+                        for (int dx = -1; dx <= 1; ++dx) {
+                            // the carried rows this x row is a neighbour of
+                            bool any = false;
 #pragma unroll
-                        for (int m = 0; m < M; ++m) {
-                            const int dy = l - m;
-                            if (dy >= -1 && dy <= 1 && st_slot<PAT>(dz, dy, dx) >= 0) any = true;
-                        }
-                        if (!any) continue;
-                        int64_t c = (int64_t)i0 + (int64_t)dz * A.S2 + (int64_t)l * S + dx;
-                        // rows that have none of these entries may point outside x:
-                        // read a valid row instead (its values are not used)
-                        c = c < 0 ? 0 : (c > last ? last : c);
-                        FX xv[VK];
-                        ld_x<FX, VK>(x + ((uint32_t)c * (uint32_t)NV + (uint32_t)k0), xv);
+                            for (int m = 0; m < M; ++m) {
+                                const int dy = l - m;
+                                if (dy >= -1 && dy <= 1 && st_slot<PAT>(dz, dy, dx) >= 0)
+                                    any = true;
+                            }
+                            if (!any) continue;
+                            int64_t c = (int64_t)i0 + (int64_t)dz * A.S2 + (int64_t)l * S + dx;
+                            // rows that have none of these entries may point
+                            // outside x: read a valid row instead (not used)
+                            if (!FAST) c = c < 0 ? 0 : (c > last ? last : c);
+                            FX xr[VK];
+                            ld_x<FX, VK>(x + ((uint32_t)c * (uint32_t)NV + (uint32_t)k0), xr);
+                            F xv[VK];
 #pragma unroll
-                        for (int m = 0; m < M; ++m) {
-                            const int dy = l - m;
-                            if (dy < -1 || dy > 1) continue;
-                            const int s = st_slot<PAT>(dz, dy, dx);
-                            if (s < 0) continue;
-                            const bool has = ((msk[m] >> s) & 1u) && !(s == CENTER && df);
-                            const F av = val_as<F, V>(vat(s, m));
+                            for (int v = 0; v < VK; ++v) xv[v] = (F)xr[v];
 #pragma unroll
-                            for (int v = 0; v < VK; ++v) {
-                                const F sum = add(y[m][v], mul((F)xv[v], av));
-                                y[m][v] = has ? sum : y[m][v];
+                            for (int m = 0; m < M; ++m) {
+                                const int dy = l - m;
+                                if (dy < -1 || dy > 1) continue;
+                                const int s = st_slot<PAT>(dz, dy, dx);
+                                if (s < 0) continue;
+                                const F av = val_as<F, V>(vb[(s * M + m) * TX]);
+                                if (FAST && s != CENTER)
+                                    st_acc<F, VK>(y[m], xv, av, true);
+                                else if (FAST)
+                                    st_acc<F, VK>(y[m], xv, av, !df);
+                                else
+                                    st_acc<F, VK>(y[m], xv, av,
+                                                  ((msk[m] >> s) & 1u) && !(s == CENTER && df));
                             }
                         }
                     }
                 }
-            }
+            };
+            if (fast)
+                body(std::true_type());
+            else
+                body(std::false_type());
             F none[1] = {F(0)};
 #pragma unroll
             for (int m = 0; m < M; ++m) {
