@@ -361,8 +361,13 @@ static void launch_stencil(const DCsr &A, const F *x, const Epi &epi, cudaStream
 // tuning on, the first SpMV without dot products for each precision and nv
 // times y = A x (EStore into a scratch y, the caller's x) with the stencil
 // kernel's two register budgets and with the CSR kernel's tuned shape (the
-// faster of two rounds of three launches each, outside any graph capture) and
-// keeps the fastest. All give the same results bit for bit.
+// faster of two rounds of three launches each, outside any graph capture).
+// A stencil form is kept only when it is at least ST_MARGIN faster than the
+// CSR kernel: the smoothers' epilogues read and write more vectors than the
+// timed y = A x, which costs the register-heavy stencil kernel more
+// (measured in the 128^3 solve: its Chebyshev steps 13 % slower than CSR at
+// equal y = A x times). All give the same results bit for bit.
+constexpr float ST_MARGIN = 0.9f;
 constexpr uint8_t ST_USE64 = 1, ST_USE128 = 2, ST_USE_CSR = 3;
 template <typename F, typename I, int NV, bool CALLER_X>
 static uint8_t tune_stencil(const DCsr &A, const F *x, cudaStream_t s) {
@@ -409,6 +414,7 @@ static uint8_t tune_stencil(const DCsr &A, const F *x, cudaStream_t s) {
             best = ms;
             code = c;
         }
+        if (c == ST_USE_CSR && code != ST_USE_CSR && best > ST_MARGIN * ms) code = ST_USE_CSR;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -205,9 +205,12 @@ __global__ void __launch_bounds__(ST_THREADS, MINB)
                     st_acc<F, VK>(y[m], xv, val_as<F, V>(vb[(CENTER * M + m) * TX]), has);
                 }
             }
+            // the plane loop stays rolled: both paths unrolled three times over
+            // overflow the instruction cache (measured: instruction-fetch
+            // stalls five times the issue rate)
             auto body = [&](auto fastc) {
                 constexpr bool FAST = decltype(fastc)::value;
-#pragma unroll
+#pragma unroll 1
                 for (int dz = -1; dz <= 1; ++dz) {
 #pragma unroll
                     for (int l = -1; l <= M; ++l) {
