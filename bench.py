@@ -69,11 +69,10 @@ def params_for(w, reduced):
         sm["max_iters"] = w["sweeps"]
     # plain: XAMG's FP64 method with XAMG's index narrowing. chosen: the whole
     # multigrid preconditioner (finest level included) in FP32 with 2-byte
-    # column offsets where they fit and a grid-stencil copy of grid operators
-    # (each SpMV takes the stencil or the CSR kernel, whichever the autotuner
-    # measured faster), and on the workloads where it measured faster the
-    # finest levels' matrix values stored in BF16 (bf16_levels); the outer
-    # iteration stays FP64.
+    # column offsets where they fit, and on the workloads where it measured
+    # faster the finest levels' matrix values stored in BF16 (bf16_levels);
+    # the outer iteration stays FP64. (The grid-stencil copy,
+    # gpu_index_compress = 3, measured slower in these solves.)
     prec = {"method": "MultiGrid", "max_iters": 1, "mg_agg_num_levels": 0,
             "mg_strength_threshold": 0.25, "mg_coarsening_type": 8,
             "mg_interpolation_type": 6, "mg_coarse_matrix_size": 500,
@@ -81,7 +80,7 @@ def params_for(w, reduced):
     solver = {"method": "MergedPBiCGStab", "max_iters": 500, "rel_tolerance": 1e-8,
               "abs_tolerance": 0, "gpu_index_compress": 1}
     if reduced:
-        prec.update(gpu_precond_f32=1, gpu_index_compress=3,
+        prec.update(gpu_precond_f32=1, gpu_index_compress=2,
                     gpu_level_bf16=w.get("bf16_levels", 0))
         solver.update(gpu_index_compress=2)
     return {"solver": solver, "preconditioner": prec,

@@ -959,6 +959,10 @@ void Krylov::solve(DVec &x, DVec &b, const std::vector<double> &conv) {
         solve_rbicgstab(x, b, conv);
         return;
     }
+    if (loop_ok() && launch_loop(x, b)) {
+        loop_done(x);
+        return;
+    }
     begin(x, b, conv);
     XG_CUDA(cudaStreamSynchronize(S()));
     if (started()) return;
@@ -976,6 +980,197 @@ void Krylov::solve(DVec &x, DVec &b, const std::vector<double> &conv) {
     XG_CUDA(cudaStreamSynchronize(S()));
 }
 
+
+// The whole solve as one graph (gpu_solve_graph): for the root solver of a
+// merged BiCGStab form, with graphs on, no per-iteration printing and no
+// persistent launch taking the solve.
+bool Krylov::loop_ok() const {
+    return cfg.gpu_solve_graph && cfg.gpu_graph && steppable() && !cfg.convergence_info &&
+           role == "solver" && !persistent_ok();
+}
+
+static void graph_check(cudaError_t e) {
+    if (e != cudaSuccess) throw Error(XAMG_ERR_CUDA, cudaGetErrorString(e));
+}
+
+// A conditional node of `type` after the capture's current dependencies on
+// stream s; the capture then depends on the new node. Returns its body.
+static cudaGraph_t add_conditional(cudaStream_t s, cudaGraphConditionalHandle h,
+                                   cudaGraphConditionalNodeType type, cudaGraphNode_t *node) {
+    cudaStreamCaptureStatus st;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    graph_check(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd));
+    XG_REQUIRE(st == cudaStreamCaptureStatusActive, XAMG_ERR_INTERNAL, "not capturing");
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = type;
+    np.conditional.size = 1;
+    graph_check(cudaGraphAddNode(node, g, deps, nd, &np));
+    graph_check(cudaStreamUpdateCaptureDependencies(s, node, 1, cudaStreamSetCaptureDependencies));
+    return np.conditional.phGraph_out[0];
+}
+
+// Records the solve graph: [r0 = b - A x; test rho0 (k_loop_start)]
+// WHILE(loop) { iteration up to its residual; test (k_loop_check);
+// IF(rest) { the rest of the iteration }; IF(last) { final x update } }.
+// The recording runs the host side of one solve (flags, pointers) without
+// running its kernels; `flags` keeps the work vectors' flags it leaves.
+bool Krylov::record_loop(LoopGraph &g, DVec &x, DVec &b) {
+    cudaStream_t s = S();
+    double *SC = sc.as<double>();
+    if (!lout.bytes) lout.alloc(k::LOOP_COUNT * sizeof(double));
+    XG_CUDA(cudaStreamSynchronize(s));
+    auto code = [](const DVec &v) { return (uint8_t)((v.zero ? 1 : 0) | (v.init ? 2 : 0)); };
+    std::vector<uint8_t> before(buf.size() + 1);
+    for (size_t i = 0; i < buf.size(); ++i) before[i] = code(buf[i]);
+    before[buf.size()] = code(x);
+    cudaGraph_t G = nullptr;
+    cudaGraph_t body = nullptr, rest = nullptr, last = nullptr;
+    bool ok = true;
+    const uint64_t l0 = g_kernel_launches;
+    capturing_ = true;
+    try {
+        graph_check(cudaGraphCreate(&G, 0));
+        k::LoopCtl c{NV, cfg.max_iters, cfg.convergence_check, cfg.abs_tol, cfg.rel_tol, 0, 0, 0};
+        graph_check(cudaGraphConditionalHandleCreate(&c.loop, G, 0, cudaGraphCondAssignDefault));
+        // start: the host side of begin(), r0 = b - A x, the test of rho0
+        graph_check(cudaStreamBeginCaptureToGraph(s, G, nullptr, nullptr, 0,
+                                                  cudaStreamCaptureModeThreadLocal));
+        reset_stats();
+        f32io = f32io_ready && static_cast<MultiGrid *>(M.get())->cfg.mg_cycle != 1;
+        run_.x = &x;
+        run_.b = &b;
+        run_.tail = false;
+        run_.iconv.assign(NV, 1.0);
+        for (auto &v : buf) {
+            v.zero = true;
+            v.init = true;
+        }
+        DVec &r0 = buf[0], &r = buf[1], &p = buf[2];
+        if (x.zero)
+            ops::group1_zero(n, b.p<double>(), r0.p<double>(), p.p<double>(), r.p<double>(), SC,
+                             NV, s);
+        else
+            ops::group1(*A, x.p<double>(), b.p<double>(), r0.p<double>(), p.p<double>(),
+                        r.p<double>(), SC, NV, s);
+        r0.zero = p.zero = r.zero = false;
+        ops::loop_start(SC, lout.as<double>(), c, s);
+        cudaGraphNode_t wn;
+        body = add_conditional(s, c.loop, cudaGraphCondTypeWhile, &wn);
+        graph_check(cudaStreamEndCapture(s, &G));
+        // the loop body
+        graph_check(cudaGraphConditionalHandleCreate(&c.rest, body, 0, cudaGraphCondAssignDefault));
+        graph_check(cudaGraphConditionalHandleCreate(&c.last, body, 0, cudaGraphCondAssignDefault));
+        graph_check(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
+                                                  cudaStreamCaptureModeThreadLocal));
+        run_.pa = M ? &buf[6] : &buf[2];
+        run_.sa = M ? &buf[7] : &buf[4];
+        in_loop_ = true;  // the residual stays on the device
+        step_body();
+        in_loop_ = false;
+        ops::loop_check(SC, lout.as<double>(), c, s);
+        cudaStreamCaptureStatus st;
+        const cudaGraphNode_t *deps = nullptr;
+        size_t nd = 0;
+        graph_check(cudaStreamGetCaptureInfo(s, &st, nullptr, nullptr, &deps, &nd));
+        std::vector<cudaGraphNode_t> check_deps(deps, deps + nd);
+        cudaGraphNode_t rn, ln;
+        rest = add_conditional(s, c.rest, cudaGraphCondTypeIf, &rn);
+        graph_check(cudaStreamUpdateCaptureDependencies(s, check_deps.data(), check_deps.size(),
+                                                        cudaStreamSetCaptureDependencies));
+        last = add_conditional(s, c.last, cudaGraphCondTypeIf, &ln);
+        graph_check(cudaStreamEndCapture(s, &body));
+        // IF(rest): the rest of a non-converged iteration
+        graph_check(cudaStreamBeginCaptureToGraph(s, rest, nullptr, nullptr, 0,
+                                                  cudaStreamCaptureModeThreadLocal));
+        step_tail();
+        graph_check(cudaStreamEndCapture(s, &rest));
+        // IF(last): the final x update
+        graph_check(cudaStreamBeginCaptureToGraph(s, last, nullptr, nullptr, 0,
+                                                  cudaStreamCaptureModeThreadLocal));
+        DVec &p2 = buf[2], &s2 = buf[4];
+        if (f32io)
+            ops::x_update(n, x.p<double>(), pa32.p<float>(), sa32.p<float>(), SC, NV, s);
+        else if (precond_form)
+            ops::x_update(n, x.p<double>(), run_.pa->p<double>(), run_.sa->p<double>(), SC, NV,
+                          s);
+        else
+            ops::x_update(n, x.p<double>(), p2.p<double>(), s2.p<double>(), SC, NV, s);
+        x.zero = false;
+        graph_check(cudaStreamEndCapture(s, &last));
+        graph_check(cudaGraphInstantiate(&g.exec, G, 0));
+    } catch (...) {
+        ok = false;
+        in_loop_ = false;
+        cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(s, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone) {
+            cudaGraph_t junk = nullptr;
+            cudaStreamEndCapture(s, &junk);
+        }
+        cudaGetLastError();
+        g.exec = nullptr;
+    }
+    capturing_ = false;
+    if (G) cudaGraphDestroy(G);
+    g.launches = g_kernel_launches - l0;
+    g_kernel_launches = l0;
+    g.flags.resize(buf.size());
+    for (size_t i = 0; i < buf.size(); ++i) g.flags[i] = code(buf[i]);
+    // the flags the solve starts from (nothing of the recording ran)
+    for (size_t i = 0; i < buf.size(); ++i) {
+        buf[i].zero = before[i] & 1;
+        buf[i].init = before[i] & 2;
+    }
+    x.zero = before[buf.size()] & 1;
+    x.init = before[buf.size()] & 2;
+    return ok;
+}
+
+// Runs the solve as one graph launch; false where it is run by steps instead
+// (its first two calls for a key, which also tune the SpMVs, and solves that
+// cannot be recorded).
+bool Krylov::launch_loop(DVec &x, DVec &b) {
+    LoopGraph &g = loop_graphs_[std::make_tuple(ctx().lane, x.p<const void>(), b.p<const void>(),
+                                                x.zero)];
+    if (g.failed || (!g.exec && g.calls++ < 2)) return false;
+    if (!g.exec && !record_loop(g, x, b)) {
+        g.failed = true;
+        return false;
+    }
+    reset_stats();
+    loop_x_zero_ = x.zero;
+    run_.x = &x;
+    run_.b = &b;
+    run_.tail = false;
+    XG_CUDA(cudaGraphLaunch(g.exec, S()));
+    g_kernel_launches += g.launches;
+    for (size_t i = 0; i < buf.size(); ++i) {
+        buf[i].zero = g.flags[i] & 1;
+        buf[i].init = g.flags[i] & 2;
+    }
+    return true;
+}
+
+// After the stream has passed a loop graph: statistics, and x's flags (x is
+// written unless rho0 passed the test already).
+void Krylov::loop_done(DVec &x) {
+    Ctx &c = ctx();
+    XG_CUDA(cudaMemcpyAsync(c.pinned, lout.p, k::LOOP_COUNT * sizeof(double),
+                            cudaMemcpyDeviceToHost, S()));
+    XG_CUDA(cudaStreamSynchronize(S()));
+    const double *o = c.pinned;
+    st.iters = (int)o[k::LOOP_ITERS];
+    for (int kk = 0; kk < NV; ++kk) {
+        st.conv[kk] = o[k::LOOP_CONV + kk] != 0.0 ? 1 : 0;
+        st.abs_res[kk] = o[k::LOOP_ABS + kk];
+        st.rel_res[kk] = o[k::LOOP_REL + kk];
+    }
+    x.zero = loop_x_zero_ && st.iters == 0;
+    x.init = true;
+}
 
 // merged_bicgstab.inl:44-208 / merged_pbicgstab.inl:44-225
 void Krylov::begin(DVec &x, DVec &b, const std::vector<double> &conv) {
@@ -1199,7 +1394,7 @@ void Krylov::step_body() {
         apply_M(sa32, s_);
         ops::spmv_dot3(*A, sa32.p<float>(), t.p<double>(), s_.p<double>(), SC, NV, s);
         t.zero = false;
-        post_scalars(SC + k::SC_RES * k::SC_STRIDE, NV);
+        if (!in_loop_) post_scalars(SC + k::SC_RES * k::SC_STRIDE, NV);
         return;
     }
     if (M) {
@@ -1219,7 +1414,7 @@ void Krylov::step_body() {
     // t = A s_; omega = (t,s)/(t,t); res = (s,s) - omega (t,s)
     ops::spmv_dot3(*A, run_.sa->p<double>(), t.p<double>(), s_.p<double>(), SC, NV, s);
     t.zero = false;
-    post_scalars(SC + k::SC_RES * k::SC_STRIDE, NV);
+    if (!in_loop_) post_scalars(SC + k::SC_RES * k::SC_STRIDE, NV);
 }
 
 bool Krylov::stepped() {
@@ -1375,11 +1570,15 @@ void solve_batch(const std::vector<SolverHierarchy *> &hs, const std::vector<DVe
         c.use_lane(i + 1);
         XG_CUDA(cudaStreamWaitEvent(c.stream, guard.ev, 0));
     }
+    // systems whose whole solve runs as one graph launch (gpu_solve_graph)
+    std::vector<char> looped(m, 0);
     for (int i = 0; i < m; ++i) {
         c.use_lane(i + 1);
         std::vector<double> ones(hs[i]->NV, 1.0);
         kr[i] = dynamic_cast<Krylov *>(hs[i]->root.get());
-        if (kr[i] && kr[i]->steppable()) {
+        if (kr[i] && kr[i]->loop_ok() && kr[i]->launch_loop(*xs[i], *bs[i])) {
+            looped[i] = 1;
+        } else if (kr[i] && kr[i]->steppable()) {
             kr[i]->begin(*xs[i], *bs[i], ones);
             live[i] = 1;
         } else {
@@ -1413,6 +1612,11 @@ void solve_batch(const std::vector<SolverHierarchy *> &hs, const std::vector<DVe
                 }
             }
     }
+    for (int i = 0; i < m; ++i)
+        if (looped[i]) {
+            c.use_lane(i + 1);
+            kr[i]->loop_done(*xs[i]);
+        }
     // join: lane 0 waits for every lane; then each lane's wait-timeout flag
     for (int i = 0; i < m; ++i) {
         c.use_lane(i + 1);

@@ -123,6 +123,20 @@ class Krylov : public SolverBase {
     // pending. started()/stepped() return true when the solve is finished;
     // finish() launches a pending rest when the solve stops at max_iters.
     bool steppable() const { return !pcg && !rbicgstab; }
+    // gpu_solve_graph (default 1): a merged BiCGStab solve from the root
+    // (every right-hand side active) as one graph launch: r0 = b - A x, the
+    // convergence test of rho0, then a device-side loop (a conditional WHILE
+    // node) over the iteration up to its residual, its convergence test (a
+    // one-thread kernel that sets the loop's conditions, csrc/loop.cu) and,
+    // as conditional IF nodes, the rest of the iteration or the final x
+    // update. The same kernels in the same order as begin/step/stepped/finish,
+    // so the same results bit for bit, without a host round trip an
+    // iteration. launch_loop() returns false where the solve cannot be
+    // recorded (it then runs the steps); loop_done() reads the statistics
+    // once the stream has passed the graph.
+    bool loop_ok() const;
+    bool launch_loop(DVec &x, DVec &b);
+    void loop_done(DVec &x);
     void begin(DVec &x, DVec &b, const std::vector<double> &conv);
     bool started();
     void step();
@@ -151,6 +165,19 @@ class Krylov : public SolverBase {
     // caller's
     std::map<std::tuple<int, bool, const void *>, MGraph> step_graphs_;
     bool capturing_ = false;  // recording step(): preconditioner runs inline
+    // whole-solve graphs per (lane, x, b, x.zero at the start)
+    struct LoopGraph {
+        cudaGraphExec_t exec = nullptr;
+        int calls = 0;        // solves run by steps before the recording
+        bool failed = false;  // not recordable: always run by steps
+        uint64_t launches = 0;
+        std::vector<uint8_t> flags;  // work vectors' zero/init after a solve
+    };
+    std::map<std::tuple<int, const void *, const void *, bool>, LoopGraph> loop_graphs_;
+    DevBuf lout;               // the loop's statistics (k::LOOP_COUNT doubles)
+    bool loop_x_zero_ = false; // x.zero when the running loop graph started
+    bool in_loop_ = false;     // recording the loop body (no host read-back)
+    bool record_loop(LoopGraph &g, DVec &x, DVec &b);
     // state of the merged BiCGStab solve between its steps
     struct Run {
         DVec *x = nullptr, *b = nullptr, *pa = nullptr, *sa = nullptr;
@@ -174,10 +201,11 @@ struct SolverHierarchy {
 
 // Solves independent systems together (XAMG_b200_solver_solve_batch): system i
 // runs on lane i + 1 (its own stream and reduction scratch), so the systems'
-// kernels run concurrently. The merged BiCGStab forms advance in lockstep:
-// every round launches one iteration of each unfinished system, then the host
-// synchronises the lanes once and tests each residual. Other methods run to
-// the end on their lane. The lanes start after the work already queued on
+// kernels run concurrently. A system whose solve runs as one graph
+// (gpu_solve_graph) is launched once and read back at the end; the other
+// merged BiCGStab forms advance in lockstep: every round launches one
+// iteration of each unfinished system, then the host synchronises the lanes
+// once and tests each residual. Other methods run to the end on their lane. The lanes start after the work already queued on
 // lane 0, and lane 0 waits for all of them before the call returns.
 void solve_batch(const std::vector<SolverHierarchy *> &hs, const std::vector<DVec *> &xs,
                  const std::vector<DVec *> &bs);
