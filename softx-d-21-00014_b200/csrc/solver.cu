@@ -1058,6 +1058,7 @@ bool Krylov::record_loop(LoopGraph &g, DVec &x, DVec &b) {
                         r.p<double>(), SC, NV, s);
         r0.zero = p.zero = r.zero = false;
         ops::loop_start(SC, lout.as<double>(), c, s);
+        g.n_start = g_kernel_launches - l0;
         cudaGraphNode_t wn;
         body = add_conditional(s, c.loop, cudaGraphCondTypeWhile, &wn);
         graph_check(cudaStreamEndCapture(s, &G));
@@ -1069,9 +1070,11 @@ bool Krylov::record_loop(LoopGraph &g, DVec &x, DVec &b) {
         run_.pa = M ? &buf[6] : &buf[2];
         run_.sa = M ? &buf[7] : &buf[4];
         in_loop_ = true;  // the residual stays on the device
+        uint64_t l1 = g_kernel_launches;
         step_body();
         in_loop_ = false;
         ops::loop_check(SC, lout.as<double>(), c, s);
+        g.n_body = g_kernel_launches - l1;
         cudaStreamCaptureStatus st;
         const cudaGraphNode_t *deps = nullptr;
         size_t nd = 0;
@@ -1086,12 +1089,15 @@ bool Krylov::record_loop(LoopGraph &g, DVec &x, DVec &b) {
         // IF(rest): the rest of a non-converged iteration
         graph_check(cudaStreamBeginCaptureToGraph(s, rest, nullptr, nullptr, 0,
                                                   cudaStreamCaptureModeThreadLocal));
+        l1 = g_kernel_launches;
         step_tail();
+        g.n_rest = g_kernel_launches - l1;
         graph_check(cudaStreamEndCapture(s, &rest));
         // IF(last): the final x update
         graph_check(cudaStreamBeginCaptureToGraph(s, last, nullptr, nullptr, 0,
                                                   cudaStreamCaptureModeThreadLocal));
         DVec &p2 = buf[2], &s2 = buf[4];
+        l1 = g_kernel_launches;
         if (f32io)
             ops::x_update(n, x.p<double>(), pa32.p<float>(), sa32.p<float>(), SC, NV, s);
         else if (precond_form)
@@ -1100,6 +1106,7 @@ bool Krylov::record_loop(LoopGraph &g, DVec &x, DVec &b) {
         else
             ops::x_update(n, x.p<double>(), p2.p<double>(), s2.p<double>(), SC, NV, s);
         x.zero = false;
+        g.n_last = g_kernel_launches - l1;
         graph_check(cudaStreamEndCapture(s, &last));
         graph_check(cudaGraphInstantiate(&g.exec, G, 0));
     } catch (...) {
@@ -1115,7 +1122,6 @@ bool Krylov::record_loop(LoopGraph &g, DVec &x, DVec &b) {
     }
     capturing_ = false;
     if (G) cudaGraphDestroy(G);
-    g.launches = g_kernel_launches - l0;
     g_kernel_launches = l0;
     g.flags.resize(buf.size());
     for (size_t i = 0; i < buf.size(); ++i) g.flags[i] = code(buf[i]);
@@ -1146,7 +1152,7 @@ bool Krylov::launch_loop(DVec &x, DVec &b) {
     run_.b = &b;
     run_.tail = false;
     XG_CUDA(cudaGraphLaunch(g.exec, S()));
-    g_kernel_launches += g.launches;
+    loop_run_ = &g;
     for (size_t i = 0; i < buf.size(); ++i) {
         buf[i].zero = g.flags[i] & 1;
         buf[i].init = g.flags[i] & 2;
@@ -1170,6 +1176,16 @@ void Krylov::loop_done(DVec &x) {
     }
     x.zero = loop_x_zero_ && st.iters == 0;
     x.init = true;
+    // the kernels the device loop ran: each iteration's body and test, then
+    // the rest of the iteration, or the final x update when it converged
+    if (loop_run_) {
+        const LoopGraph &g = *loop_run_;
+        const uint64_t it = (uint64_t)st.iters;
+        const bool done = o[k::LOOP_DONE] != 0.0;
+        g_kernel_launches += g.n_start + it * g.n_body;
+        if (it) g_kernel_launches += done ? (it - 1) * g.n_rest + g.n_last : it * g.n_rest;
+        loop_run_ = nullptr;
+    }
 }
 
 // merged_bicgstab.inl:44-208 / merged_pbicgstab.inl:44-225

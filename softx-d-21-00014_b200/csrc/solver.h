@@ -170,12 +170,15 @@ class Krylov : public SolverBase {
         cudaGraphExec_t exec = nullptr;
         int calls = 0;        // solves run by steps before the recording
         bool failed = false;  // not recordable: always run by steps
-        uint64_t launches = 0;
+        // kernels of the start, of one pass of the loop body (iteration and
+        // test), of the rest of an iteration and of the final x update
+        uint64_t n_start = 0, n_body = 0, n_rest = 0, n_last = 0;
         std::vector<uint8_t> flags;  // work vectors' zero/init after a solve
     };
     std::map<std::tuple<int, const void *, const void *, bool>, LoopGraph> loop_graphs_;
     DevBuf lout;               // the loop's statistics (k::LOOP_COUNT doubles)
     bool loop_x_zero_ = false; // x.zero when the running loop graph started
+    const LoopGraph *loop_run_ = nullptr;  // the loop graph launched last
     bool in_loop_ = false;     // recording the loop body (no host read-back)
     bool record_loop(LoopGraph &g, DVec &x, DVec &b);
     // state of the merged BiCGStab solve between its steps

@@ -3,7 +3,8 @@ benchmark description's configuration 4 at 32^3): training pairs from the
 solver, the MLP trained on the GPU (its loss must fall at least tenfold), and
 held-out solves from the zero guess and from the learned guess, which is kept
 per right-hand side only when its initial residual is below the zero guess's.
-Both must converge; with the guess the iteration count must not grow."""
+Both must converge; the guess must be kept for most right-hand sides, at
+least halve the initial residual, and not add iterations."""
 import os
 import sys
 
@@ -20,5 +21,8 @@ def test_learned_guess_pipeline(gpu):
                       log=lambda *a: None)
     assert out["final_loss"] < out["first_loss"] / 10
     assert out["learned_iters"] <= out["zero_iters"]
-    assert 0.0 <= out["guesses_kept"] <= 1.0
-    assert out["initial_residual_ratio"] <= 1.0
+    # the smoothed guess of the trained network passes the acceptance test
+    # for most held-out right-hand sides and at least halves their initial
+    # residual (measured: all kept, 0.20 of the zero guess's residual)
+    assert out["guesses_kept"] >= 0.5
+    assert out["initial_residual_ratio"] <= 0.5
