@@ -907,6 +907,13 @@ int XAMG_b200_solver_level_stencil(size_t sid, int level, int which, int *patter
     });
 }
 
+int XAMG_b200_solver_level_xstaged(size_t sid, int level, int which, int *nv) {
+    return guarded([&] {
+        XG_REQUIRE(nv, XAMG_ERR_INVALID_ARG, "null pointer");
+        *nv = level_matrix(sid, level, which).xs_nv;
+    });
+}
+
 int XAMG_b200_solver_level_tuned(size_t sid, int level, int which, uint8_t *codes) {
     return guarded([&] {
         XG_REQUIRE(codes, XAMG_ERR_INVALID_ARG, "null array");

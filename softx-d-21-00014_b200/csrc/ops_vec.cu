@@ -393,11 +393,54 @@ static void upload_stencil(const HCsr &h, DCsr &d, cudaStream_t s) {
     d.st_diag_first = df;
 }
 
+// The x-staged copy (csrc/xstage.cuh) for nv right-hand sides: rows of at
+// least 16 entries on average, at least 4,096 of them, a tile's x rows and
+// staged entries within 96 KB of shared memory, at most 65,535 unique columns
+// a tile.
+static void upload_xstage(const HCsr &h, DCsr &d, int nv, cudaStream_t s) {
+    const uint64_t n = h.nrows, nnz = h.nnz();
+    if (nv < 1 || n < 4096 || nnz < 16 * n) return;
+    const uint64_t R = (uint64_t)k::CT / (uint64_t)nv;
+    const uint64_t ntiles = (n + R - 1) / R;
+    std::vector<uint32_t> uptr(ntiles + 1, 0), ucol;
+    std::vector<uint16_t> slot(nnz);
+    ucol.reserve(nnz / 2);
+    uint32_t umax = 0, emax = 0;
+    std::vector<uint32_t> cols;
+    for (uint64_t t = 0; t < ntiles; ++t) {
+        const uint64_t r0 = t * R, r1 = std::min(n, r0 + R);
+        const uint32_t j0 = h.row[r0], j1 = h.row[r1];
+        cols.assign(h.col.begin() + j0, h.col.begin() + j1);
+        std::sort(cols.begin(), cols.end());
+        cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+        if (cols.size() > 65535) return;
+        for (uint32_t j = j0; j < j1; ++j)
+            slot[j] = (uint16_t)(std::lower_bound(cols.begin(), cols.end(), h.col[j]) - cols.begin());
+        ucol.insert(ucol.end(), cols.begin(), cols.end());
+        uptr[t + 1] = (uint32_t)ucol.size();
+        umax = std::max<uint32_t>(umax, (uint32_t)cols.size());
+        emax = std::max<uint32_t>(emax, j1 - j0);
+    }
+    const uint32_t xsz = d.f32 ? 4 : 8, vsz = d.bf16 ? 2 : xsz;
+    auto r16 = [](uint64_t b) { return (b + 15) & ~(uint64_t)15; };
+    const uint64_t smem = r16((uint64_t)umax * nv * xsz) + r16((uint64_t)emax * vsz + 32) +
+                          r16((uint64_t)emax * 2 + 32);
+    if (smem > 96 * 1024) return;
+    upload(d.xs_uptr, uptr, s);
+    upload(d.xs_ucol, ucol, s);
+    upload(d.xs_slot, slot, s);
+    XG_CUDA(cudaStreamSynchronize(s));
+    d.xs_nv = nv;
+    d.xs_umax = umax;
+    d.xs_emax = emax;
+}
+
 void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s, int tune,
-                bool bf16) {
+                bool bf16, int xs_nv) {
     d.tune_on = tune == 1;
     d.st_force = tune == 2 ? 2 : 0;
     d.wide_force = tune == 3;
+    d.xs_force = tune == 4;
     d.bf16 = f32 && bf16;
     d.nrows = h.nrows;
     d.ncols = h.ncols;
@@ -465,6 +508,11 @@ void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s, in
     d.st_val.release();
     d.st_mask.release();
     if (narrow >= 3) upload_stencil(h, d, s);
+    d.xs_nv = 0;
+    d.xs_uptr.release();
+    d.xs_ucol.release();
+    d.xs_slot.release();
+    if (narrow >= 2 && xs_nv > 0) upload_xstage(h, d, xs_nv, s);
     XG_CUDA(cudaStreamSynchronize(s));
 }
 

@@ -84,7 +84,8 @@ struct SolverCfg {
     int gpu_graph = 1;          // replay preconditioner applications as CUDA graphs
     int gpu_spmv_tune = 1;      // SpMV launch shapes picked by measurement (2: no tuning,
                                 // the grid-stencil kernel's 128-register form; 3: no
-                                // tuning, the warp-per-row kernel on small matrices)
+                                // tuning, the warp-per-row kernel on small matrices;
+                                // 4: no tuning, the x-staged kernel where built)
     int gpu_level_bf16 = 0;     // finest FP32 cycle levels whose matrix values are BF16
     int gpu_seed = 0;           // seed of the host setup's random choices
     int gpu_persistent = 1;     // eligible BiCGStab solves in one cooperative launch

@@ -528,7 +528,7 @@ void MultiGrid::build(const HCsr &A0, const DCsr *A0dev, const Params &P, const 
         // BF16 values (the smoothers' diagonals stay float from the exact values)
         if (l >= 1 || full32)
             upload_csr(HH.lv[l].A, lv.A, lv.f32, narrow, S(), tune,
-                       lv.f32 && l < cfg.gpu_level_bf16);
+                       lv.f32 && l < cfg.gpu_level_bf16, nv);
         if (l + 1 < nl) {
             // R = P^T (hypre_base.inl:400-401, transpose.inl:31-108)
             const HCsr &Ph = HH.lv[l].P;
@@ -549,8 +549,8 @@ void MultiGrid::build(const HCsr &A0, const DCsr *A0dev, const Params &P, const 
                     R.val[pos[c]] = Ph.val[j];
                     ++pos[c];
                 }
-            upload_csr(Ph, lv.P, lv.tf32, narrow, S(), tune);
-            upload_csr(R, lv.R, lv.tf32, narrow, S(), tune);
+            upload_csr(Ph, lv.P, lv.tf32, narrow, S(), tune, false, nv);
+            upload_csr(R, lv.R, lv.tf32, narrow, S(), tune, false, nv);
         }
         const uint64_t nrow = HH.lv[l].A.nrows;
         if (l == 0) {

@@ -10,6 +10,7 @@
 
 #include "ops.h"
 #include "stencil.cuh"
+#include "xstage.cuh"
 
 namespace xg {
 namespace ops {
@@ -153,7 +154,45 @@ static void launch_wide(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t
     XG_CUDA(cudaGetLastError());
     ++g_kernel_launches;
 }
+// The x-staged kernel (k_spmv_xs) on a matrix's x-staged copy for NV: one
+// wave of persistent blocks over the canonical tiles.
+template <typename F, typename FX, int NV, typename V, class Epi>
+static void launch_xs(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s) {
+    constexpr int VK = k::spmv_vk<FX, NV>();
+    constexpr int NT = k::CT / VK;
+    XG_REQUIRE(std::max(A.ncols, A.nrows) * (uint64_t)NV < (1ull << 32), XAMG_ERR_UNSUPPORTED,
+               "SpMV: x of 2^32 or more values");
+    auto kern = k::k_spmv_xs<F, FX, NV, VK, Epi, V>;
+    const uint32_t smem = k::xs_smem_bytes<FX, V, NV>(A.xs_umax, A.xs_emax);
+    static uint32_t attr = 48 * 1024;  // dynamic shared memory allowed so far (per instantiation)
+    if (smem > attr) {
+        XG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     96 * 1024));
+        attr = 96 * 1024;
+    }
+    const int res = resident_blocks(kern, NT, smem);
+    const uint64_t R = k::CT / NV;
+    const uint64_t ntiles = (A.nrows + R - 1) / R;
+    const uint32_t P = (uint32_t)std::min<uint64_t>(ntiles, (uint64_t)res * ctx().sms);
+    const k::XsArgs xa{A.xs_uptr.as<uint32_t>(), A.xs_ucol.as<uint32_t>(),
+                       A.xs_slot.as<uint16_t>(), A.xs_umax, A.xs_emax};
+    kern<<<P, NT, smem, s>>>(A.args<F>(), xa, x, epi, ctx().red().flag);
+    XG_CUDA(cudaGetLastError());
+    ++g_kernel_launches;
+}
+
+// Whether the x-staged kernel can take this SpMV: a copy built for NV, x
+// aligned for its vector loads, the block's shared memory within 96 KB (an
+// x type wider than the level's, as in the FP64-to-FP32 restriction, needs
+// more than the upload checked).
+template <typename FX, typename V, int NV>
+static bool xs_usable(const DCsr &A, const FX *x) {
+    return A.xs_nv == NV && (uintptr_t)x % (k::spmv_vk<FX, NV>() * sizeof(FX)) == 0 &&
+           k::xs_smem_bytes<FX, V, NV>(A.xs_umax, A.xs_emax) <= 96u * 1024u;
+}
+
 constexpr uint8_t TUNE_WIDE = 19;         // autotuner code of the warp-per-row kernel
+constexpr uint8_t TUNE_XS = 20;           // ... of the x-staged kernel
 constexpr uint64_t WIDE_MAX_VALUES = 1u << 20;  // rows * nv up to which it is a candidate
 
 // Autotuner of the SpMVs without dot products: the right-hand sides a thread
@@ -164,7 +203,8 @@ constexpr uint64_t WIDE_MAX_VALUES = 1u << 20;  // rows * nv up to which it is a
 // timed with CUDA events on the caller's x into a scratch y (EStore), once
 // per matrix, precision and nv, outside any graph capture; the fastest is
 // kept in the matrix (DCsr::tuned). Matrices of at most WIDE_MAX_VALUES rows
-// times nv also time the warp-per-row kernel (code TUNE_WIDE). Every candidate
+// times nv also time the warp-per-row kernel (code TUNE_WIDE), and matrices
+// with an x-staged copy for nv the x-staged kernel (code TUNE_XS). Every candidate
 // sums each (row, right-hand side) in the same CSR order, so the choice never
 // changes a result.
 constexpr uint32_t TUNE_RUNS[3] = {1, 4, 16};
@@ -223,6 +263,24 @@ static uint8_t autotune(const DCsr &A, const FX *x, cudaStream_t s) {
                     code = (uint8_t)(1 + alt * 9 + (nb - 1) * 3 + ri);
                 }
             }
+    if (xs_usable<FX, V, NV>(A, x)) {
+        auto go = [&] { launch_xs<F, FX, NV, V>(A, x, e, s); };
+        float ms = 1e30f;
+        go();
+        for (int round = 0; round < 2; ++round) {
+            XG_CUDA(cudaEventRecord(e0, s));
+            for (int r = 0; r < 3; ++r) go();
+            XG_CUDA(cudaEventRecord(e1, s));
+            XG_CUDA(cudaEventSynchronize(e1));
+            float t = 0;
+            XG_CUDA(cudaEventElapsedTime(&t, e0, e1));
+            ms = std::min(ms, t);
+        }
+        if (ms < best) {
+            best = ms;
+            code = TUNE_XS;
+        }
+    }
     if (A.nrows * (uint64_t)NV <= WIDE_MAX_VALUES) {
         auto go = [&] { launch_wide<F, FX, I, NV, V>(A, x, e, s); };
         float ms = 1e30f;
@@ -268,6 +326,10 @@ static void launch_v(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s)
             launch_wide<F, FX, I, NV, V>(A, x, epi, s);
             return;
         }
+        if (A.xs_force && xs_usable<FX, V, NV>(A, x)) {
+            launch_xs<F, FX, NV, V>(A, x, epi, s);
+            return;
+        }
     }
     if constexpr (NRED == 0 && NV > 1) {
         if (A.tune_on && (uintptr_t)x % (4 * sizeof(FX)) == 0) {
@@ -277,6 +339,10 @@ static void launch_v(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s)
             if (!t) t = autotune<F, FX, I, NV, V>(A, x, s);
             if (t == TUNE_WIDE) {
                 launch_wide<F, FX, I, NV, V>(A, x, epi, s);
+                return;
+            }
+            if (t == TUNE_XS && xs_usable<FX, V, NV>(A, x)) {
+                launch_xs<F, FX, NV, V>(A, x, epi, s);
                 return;
             }
             if (t) {

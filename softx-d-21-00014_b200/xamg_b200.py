@@ -62,6 +62,7 @@ EXT_SYMBOLS = [
     "XAMG_b200_mlp_destroy", "XAMG_b200_mlp_predict", "XAMG_b200_mlp_train_step",
     "XAMG_b200_mlp_gradients", "XAMG_b200_mlp_params", "XAMG_b200_solver_solve_batch",
     "XAMG_b200_solver_level_tuned", "XAMG_b200_stencil_layout", "XAMG_b200_solver_level_stencil",
+    "XAMG_b200_solver_level_xstaged",
 ]
 
 
@@ -201,6 +202,8 @@ def lib():
         "XAMG_b200_matrix_hierarchy_load": (C.c_int, [C.c_size_t, C.c_char_p]),
         "XAMG_b200_solver_solve_batch": (C.c_int, [C.c_int, vp, vp, vp, vp]),
         "XAMG_b200_solver_level_tuned": (C.c_int, [C.c_size_t, C.c_int, C.c_int, vp]),
+        "XAMG_b200_solver_level_xstaged": (C.c_int, [C.c_size_t, C.c_int, C.c_int,
+                                                     C.POINTER(C.c_int)]),
         "XAMG_b200_stencil_layout": (C.c_int, [u64, vp, vp, C.POINTER(C.c_int),
                                                C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
                                                C.POINTER(C.c_int)]),
@@ -532,6 +535,12 @@ class Solver:
         out = np.zeros(24, np.uint8)
         call("XAMG_b200_solver_level_tuned", self.h, level, which, _ptr(out))
         return out.reshape(2, 2, 6)
+
+    def level_xstaged(self, level, which):
+        """The nv the level matrix's x-staged copy was built for (0: none)."""
+        v = C.c_int()
+        call("XAMG_b200_solver_level_xstaged", self.h, level, which, C.byref(v))
+        return v.value
 
     def level_stencil(self, level, which):
         """The level matrix's grid-stencil copy: (pattern, S, S2, diag_first),

@@ -178,3 +178,60 @@ def test_warp_per_row_kernel_bit_exact(gpu, oracle, nv, f32):
     v = val.astype(np.float32) if f32 else val
     assert y.tobytes() == oracle.csr_ax_y(row, col, v, xh, nv).tobytes()
     assert ya.tobytes() == oracle.csr_ax_y(row, col, v, xh, nv, axpy_y=y0).tobytes()
+
+
+@pytest.mark.parametrize("nv", [1, 2, 8, 32])
+@pytest.mark.parametrize("bf16", [False, True])
+def test_x_staged_kernel_bit_exact(gpu, oracle, nv, bf16):
+    """The x-staged SpMV (gpu_spmv_tune = 4; an autotuner candidate on
+    multigrid levels with long rows): each tile's x rows copied once into
+    shared memory by unique column, each row summed from there in entry
+    order. Every element equals the oracle's sequential row sum, for y = A x
+    and y += A x, on the FP32 cycle operator (FP32 or BF16 values)."""
+    row, col, val = banded_plus_random(6000, 0, 20, seed=nv + 70)
+    params = {"solver": {"method": "MergedPBiCGStab", "rel_tolerance": 1e-8, "max_iters": 5,
+                         "gpu_index_compress": 2},
+              "preconditioner": {"method": "MultiGrid", "mg_max_levels": 2,
+                                 "mg_coarsening_type": 8, "mg_interpolation_type": 6,
+                                 "mg_agg_num_levels": 0, "gpu_precond_f32": 1,
+                                 "gpu_index_compress": 2, "gpu_spmv_tune": 4,
+                                 "gpu_level_bf16": 1 if bf16 else 0},
+              "pre_smoother": {"method": "Jacobi"}, "post_smoother": {"method": "Jacobi"}}
+    _, _, _, S = solver_on(gpu, row, col, val, nv, params)
+    assert S.level_xstaged(0, 3) == nv
+    xh, y0, y, ya = run_level_spmv(gpu, S, 0, 3, row, col, val, nv, True, seed=nv)
+    v = bf16_round(val) if bf16 else val.astype(np.float32)
+    assert y.tobytes() == oracle.csr_ax_y(row, col, v, xh, nv).tobytes()
+    assert ya.tobytes() == oracle.csr_ax_y(row, col, v, xh, nv, axpy_y=y0).tobytes()
+
+
+@pytest.mark.parametrize("tune", [1, 4])
+def test_x_staged_solves_same_bits(gpu, tune):
+    """Whole FP32-preconditioned solves on a 27-point matrix whose second
+    level gets an x-staged copy: the same bits as without tuning."""
+    row, col, val = gpu.generate_diffusion(27, 40, 40, 40, 1.0, 1.0, 8)
+    nv = 8
+    n = len(row) - 1
+    b = np.random.default_rng(33).uniform(-1, 1, n * nv)
+    out = {}
+    for t in (0, tune):
+        params = {"solver": {"method": "MergedPBiCGStab", "max_iters": 100,
+                             "rel_tolerance": 1e-8, "abs_tolerance": 0,
+                             "gpu_index_compress": 2},
+                  "preconditioner": {"method": "MultiGrid", "mg_coarsening_type": 8,
+                                     "mg_interpolation_type": 6, "mg_agg_num_levels": 0,
+                                     "mg_coarse_matrix_size": 500, "gpu_precond_f32": 1,
+                                     "gpu_index_compress": 2, "gpu_spmv_tune": t},
+                  "pre_smoother": {"method": "Chebyshev"},
+                  "post_smoother": {"method": "Chebyshev"},
+                  "coarse_grid_solver": {"method": "Direct"}}
+        M, xv, bv, S = solver_on(gpu, row, col, val, nv, params)
+        bv.upload(b)
+        for _ in range(2):
+            xv.set(0.0)
+            S.solve()
+        if t:
+            assert S.level_xstaged(1, 3) == nv
+        out[t] = (xv.download(), S.stats()["iters"])
+    assert out[0][0].tobytes() == out[tune][0].tobytes()
+    assert out[0][1] == out[tune][1]
