@@ -142,8 +142,7 @@ int XAMG_b200_solver_level_info(size_t sid, int level, int which, uint64_t *nrow
  * float x, 1 the other one) + 3 * (staging: 0 one buffer, 1 two, 2 none) +
  * (consecutive tiles a block takes: 0 one, 1 four, 2 sixteen), or 19: one warp per row (its
  * gathers in flight together, products summed in entry order; a candidate for matrices of at
- * most 2^20 rows times nv), or 20: the x-staged kernel (each tile's x rows copied once into
- * shared memory by unique column; multigrid levels with gpu_index_compress >= 2). Only SpMVs without dot products are tuned; every shape gives the
+ * most 2^20 rows times nv). Only SpMVs without dot products are tuned; every shape gives the
  * same results bit for bit. */
 int XAMG_b200_solver_level_tuned(size_t sid, int level, int which, uint8_t *codes);
 
@@ -161,10 +160,11 @@ int XAMG_b200_solver_level_tuned(size_t sid, int level, int which, uint8_t *code
  * XAMG_b200_solver_level_stencil reports a level matrix's copy (pattern -1:
  * none). */
 /* The nv a level matrix's x-staged copy was built for (0: none; no
- * counterpart). Multigrid levels uploaded with gpu_index_compress >= 2 get one
- * when their rows average at least 16 entries, they have at least 4,096 rows
- * and a tile's x rows fit in shared memory; the autotuner (or gpu_spmv_tune =
- * 4) then may run their SpMVs on it. */
+ * counterpart). With gpu_spmv_tune = 4 (and gpu_index_compress >= 2),
+ * multigrid levels whose rows average at least 16 entries, with at least 4,096
+ * rows and a tile's x rows within shared memory, get one, and their SpMVs
+ * without dot products run the x-staged kernel (each tile's x rows copied once
+ * into shared memory by unique column; the same results bit for bit). */
 int XAMG_b200_solver_level_xstaged(size_t sid, int level, int which, int *nv);
 int XAMG_b200_stencil_layout(uint64_t nrows, const uint32_t *row, const uint32_t *col,
                              int *pattern, uint32_t *S, uint32_t *S2, int *diag_first);

@@ -161,9 +161,10 @@ struct DCsr {
     uint8_t st_force = 0;     // gpu_spmv_tune = 2: always the 128-register form
     bool wide_force = false;  // gpu_spmv_tune = 3: the warp-per-row kernel where allowed
     bool xs_force = false;    // gpu_spmv_tune = 4: the x-staged kernel where built
-    // x-staged copy (gpu_index_compress >= 2 on multigrid levels,
-    // csrc/xstage.cuh), built for one nv: per canonical tile of 256/nv rows
-    // its sorted unique columns, and every entry's slot among them
+    // x-staged copy (gpu_spmv_tune = 4 with gpu_index_compress >= 2 on
+    // multigrid levels, csrc/xstage.cuh), built for one nv: per canonical
+    // tile of 256/nv rows its sorted unique columns, and every entry's slot
+    // among them
     int xs_nv = 0;  // 0: none
     uint32_t xs_umax = 0, xs_emax = 0;
     DevBuf xs_uptr, xs_ucol, xs_slot;
@@ -190,9 +191,9 @@ struct DCsr {
 // warp-per-row kernel.
 // bf16 (with f32): store the values rounded to float and then to BF16
 // (round to nearest even), the arithmetic staying in float.
-// xs_nv (narrow >= 2): also build the x-staged copy for SpMVs with xs_nv
-// right-hand sides, where the rows are long enough and a tile's x rows fit
-// in shared memory.
+// xs_nv (narrow >= 2, tune = 4): also build the x-staged copy for SpMVs with
+// xs_nv right-hand sides, where the rows are long enough and a tile's x rows
+// fit in shared memory.
 void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s, int tune = 0,
                 bool bf16 = false, int xs_nv = 0);
 void download_csr(const DCsr &d, uint32_t *row, void *col, void *val);

@@ -512,7 +512,9 @@ void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s, in
     d.xs_uptr.release();
     d.xs_ucol.release();
     d.xs_slot.release();
-    if (narrow >= 2 && xs_nv > 0) upload_xstage(h, d, xs_nv, s);
+    // only where asked for (gpu_spmv_tune = 4): measured slower than the CSR
+    // kernel on the benchmark's levels, and its host preprocessing costs setup
+    if (narrow >= 2 && xs_nv > 0 && tune == 4) upload_xstage(h, d, xs_nv, s);
     XG_CUDA(cudaStreamSynchronize(s));
 }
 

@@ -192,7 +192,6 @@ static bool xs_usable(const DCsr &A, const FX *x) {
 }
 
 constexpr uint8_t TUNE_WIDE = 19;         // autotuner code of the warp-per-row kernel
-constexpr uint8_t TUNE_XS = 20;           // ... of the x-staged kernel
 constexpr uint64_t WIDE_MAX_VALUES = 1u << 20;  // rows * nv up to which it is a candidate
 
 // Autotuner of the SpMVs without dot products: the right-hand sides a thread
@@ -203,8 +202,7 @@ constexpr uint64_t WIDE_MAX_VALUES = 1u << 20;  // rows * nv up to which it is a
 // timed with CUDA events on the caller's x into a scratch y (EStore), once
 // per matrix, precision and nv, outside any graph capture; the fastest is
 // kept in the matrix (DCsr::tuned). Matrices of at most WIDE_MAX_VALUES rows
-// times nv also time the warp-per-row kernel (code TUNE_WIDE), and matrices
-// with an x-staged copy for nv the x-staged kernel (code TUNE_XS). Every candidate
+// times nv also time the warp-per-row kernel (code TUNE_WIDE). Every candidate
 // sums each (row, right-hand side) in the same CSR order, so the choice never
 // changes a result.
 constexpr uint32_t TUNE_RUNS[3] = {1, 4, 16};
@@ -263,24 +261,6 @@ static uint8_t autotune(const DCsr &A, const FX *x, cudaStream_t s) {
                     code = (uint8_t)(1 + alt * 9 + (nb - 1) * 3 + ri);
                 }
             }
-    if (xs_usable<FX, V, NV>(A, x)) {
-        auto go = [&] { launch_xs<F, FX, NV, V>(A, x, e, s); };
-        float ms = 1e30f;
-        go();
-        for (int round = 0; round < 2; ++round) {
-            XG_CUDA(cudaEventRecord(e0, s));
-            for (int r = 0; r < 3; ++r) go();
-            XG_CUDA(cudaEventRecord(e1, s));
-            XG_CUDA(cudaEventSynchronize(e1));
-            float t = 0;
-            XG_CUDA(cudaEventElapsedTime(&t, e0, e1));
-            ms = std::min(ms, t);
-        }
-        if (ms < best) {
-            best = ms;
-            code = TUNE_XS;
-        }
-    }
     if (A.nrows * (uint64_t)NV <= WIDE_MAX_VALUES) {
         auto go = [&] { launch_wide<F, FX, I, NV, V>(A, x, e, s); };
         float ms = 1e30f;
@@ -339,10 +319,6 @@ static void launch_v(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s)
             if (!t) t = autotune<F, FX, I, NV, V>(A, x, s);
             if (t == TUNE_WIDE) {
                 launch_wide<F, FX, I, NV, V>(A, x, epi, s);
-                return;
-            }
-            if (t == TUNE_XS && xs_usable<FX, V, NV>(A, x)) {
-                launch_xs<F, FX, NV, V>(A, x, epi, s);
                 return;
             }
             if (t) {
