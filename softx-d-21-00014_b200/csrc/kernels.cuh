@@ -1394,6 +1394,7 @@ struct PersistArgs {
     float abs_tol, rel_tol;
     RedArgs ra;        // partial sums: two halves used in turn
     GridSync gs;
+    uint32_t B;        // canonical blocks (canon_blocks(n, NV)); the grid may be smaller
 };
 
 // A BiCGStab solve recorded as one graph (csrc/loop.cu): the convergence
@@ -1413,9 +1414,11 @@ constexpr int LOOP_ABS = 0, LOOP_REL = 32, LOOP_CONV = 64, LOOP_ITERS = 96, LOOP
 // merged_pbicgstab.inl:44-225 after its start (r0, rho0, p = r = r0 and the
 // first test, done by Krylov::begin/started): every iteration, its
 // convergence test (solver.h:173-241 with float32 tolerances) and the final
-// x update in one cooperative launch of B = canon_blocks(n, NV) blocks of 256
-// threads, block b being canonical block b (grid barriers between the
-// steps). Each step applies the same element operations, row sums and
+// x update in one cooperative launch of 256-thread blocks (grid barriers
+// between the steps). Physical block p plays canonical blocks p, p + grid,
+// ... of the B = canon_blocks(n, NV) (a grid smaller than B has fewer
+// blocks at each barrier); every reduction is summed per canonical block in
+// tile order. Each step applies the same element operations, row sums and
 // canonical reductions as the separate kernels of Krylov::step_tail,
 // step_body and stepped, so the iterates are the same bit for bit.
 template <int NV, typename I>
@@ -1425,7 +1428,7 @@ __global__ void __launch_bounds__(CT, 1) k_pbicgstab_persist(CsrArgs<double> A, 
     __shared__ double st_abs[NV], st_rel[NV];
     __shared__ int st_conv[NV];
     __shared__ int go;
-    const uint32_t B = gridDim.x;
+    const uint32_t B = P.B;
     const uint64_t n = A.n;
     const uint64_t ntiles = (n + R - 1) / R;
     const int rt = threadIdx.x / NV, kk = threadIdx.x % NV;
@@ -1443,12 +1446,15 @@ __global__ void __launch_bounds__(CT, 1) k_pbicgstab_persist(CsrArgs<double> A, 
     const size_t HALF = (size_t)B * NV * 4;
     auto part = [&]() { return (double *)P.ra.part + (size_t)half * HALF; };
     // every (row, right-hand side) this thread owns: canonical thread
-    // threadIdx.x of canonical block blockIdx.x, tiles in order
-    auto each = [&](auto &&fn) {
-        for (uint64_t tile = blockIdx.x; tile < ntiles; tile += B) {
+    // threadIdx.x of the canonical blocks this block plays, tiles in order
+    auto each_of = [&](uint64_t cb, auto &&fn) {
+        for (uint64_t tile = cb; tile < ntiles; tile += B) {
             const uint64_t i = tile * R + rt;
             if (i < n) fn(i, (uint64_t)i * NV + kk);
         }
+    };
+    auto each = [&](auto &&fn) {
+        for (uint64_t cb = blockIdx.x; cb < B; cb += gridDim.x) each_of(cb, fn);
     };
     // x written by other blocks in this launch: read through L2 (ld.cg), not
     // from a possibly stale L1 line
@@ -1458,10 +1464,19 @@ __global__ void __launch_bounds__(CT, 1) k_pbicgstab_persist(CsrArgs<double> A, 
             y = add(y, mul(ld_cg(&xv[col_at<I>(__ldg(&col[j]), i) * NV + kk]), __ldg(&val[j])));
         return y;
     };
-    auto sync = [&]() { return grid_sync(P.gs, B); };
-    auto reduce = [&](auto &acc, auto &&fin) {
+    auto sync = [&]() { return grid_sync(P.gs, gridDim.x); };
+    // elem(i, e, acc) over every (row, right-hand side) this block owns,
+    // summed per canonical block in tile order; then the grid's partials
+    // summed in canonical order by every block (fin writes the scalars)
+    auto reduce_each = [&](auto &acc, auto &&elem, auto &&fin) {
         constexpr int NR = sizeof(acc[0]) / sizeof(double);
-        canon_partial<double, NV, NR, 1>(acc, RedArgs{part(), nullptr, nullptr}, blockIdx.x);
+        for (uint64_t cb = blockIdx.x; cb < B; cb += gridDim.x) {
+#pragma unroll
+            for (int r = 0; r < NR; ++r) acc[0][r] = 0.0;
+            each_of(cb, [&](uint64_t i, uint64_t e) { elem(i, e, acc[0]); });
+            canon_partial<double, NV, NR, 1>(acc, RedArgs{part(), nullptr, nullptr},
+                                             (uint32_t)cb);
+        }
         if (!sync()) return false;
         canon_final_local<NV, NR>(part(), B, fin);
         half ^= 1u;
@@ -1499,8 +1514,9 @@ __global__ void __launch_bounds__(CT, 1) k_pbicgstab_persist(CsrArgs<double> A, 
     const OpPUpdate pu{P.p, P.r, P.v, SCS, NV};
     auto do_tail = [&]() {
         double acc[1][1] = {{0.0}};
-        each([&](uint64_t i, uint64_t) { g4.elem(i, kk, acc[0]); });
-        if (!reduce(acc, g4)) return false;
+        if (!reduce_each(acc, [&](uint64_t i, uint64_t, double(&a)[1]) { g4.elem(i, kk, a); },
+                         g4))
+            return false;
         each([&](uint64_t, uint64_t e) { pu(e); });
         return true;
     };
@@ -1512,8 +1528,13 @@ __global__ void __launch_bounds__(CT, 1) k_pbicgstab_persist(CsrArgs<double> A, 
         {   // v = A p_; alpha = rho / (v, r0)
             const EDotAlpha<NV> ea{P.v, P.r0, SCS};
             double acc[1][1] = {{0.0}};
-            each([&](uint64_t i, uint64_t) { ea.store(i, kk, rowsum(P.pa, i), acc[0]); });
-            if (!(ok = reduce(acc, ea))) break;
+            if (!(ok = reduce_each(
+                      acc,
+                      [&](uint64_t i, uint64_t, double(&a)[1]) {
+                          ea.store(i, kk, rowsum(P.pa, i), a);
+                      },
+                      ea)))
+                break;
         }
         {   // s = r - alpha v
             const OpSUpdate su{P.s, P.r, P.v, SCS, NV};
@@ -1524,8 +1545,13 @@ __global__ void __launch_bounds__(CT, 1) k_pbicgstab_persist(CsrArgs<double> A, 
         {   // t = A s_; omega, res
             const EDot3<NV> e3{P.t, P.s, SCS};
             double acc[1][3] = {{0.0, 0.0, 0.0}};
-            each([&](uint64_t i, uint64_t) { e3.store(i, kk, rowsum(P.sa, i), acc[0]); });
-            if (!(ok = reduce(acc, e3))) break;
+            if (!(ok = reduce_each(
+                      acc,
+                      [&](uint64_t i, uint64_t, double(&a)[3]) {
+                          e3.store(i, kk, rowsum(P.sa, i), a);
+                      },
+                      e3)))
+                break;
         }
         // convergence test (host_converged): every block decides alike
         if (threadIdx.x == 0) {

@@ -16,8 +16,10 @@ void wait_selftest(uint64_t limit_ns, cudaStream_t s);
 
 // The persistent preconditioned BiCGStab (csrc/persist.cu): whether the
 // matrix's canonical blocks can all be resident at once, and the launch.
-bool pbicgstab_persist_fits(const DCsr &A, int nv);
-void pbicgstab_persist(const DCsr &A, const k::PersistArgs &P, int nv, cudaStream_t s);
+// share: canonical blocks each physical block plays (gpu_persistent).
+bool pbicgstab_persist_fits(const DCsr &A, int nv, int share);
+void pbicgstab_persist(const DCsr &A, const k::PersistArgs &P, int nv, int share,
+                       cudaStream_t s);
 // A grid barrier that one block never reaches: its waits run out after
 // limit_ns and raise *flag.
 void grid_selftest(unsigned *count_gen, unsigned *flag, uint64_t limit_ns, cudaStream_t s);

@@ -79,7 +79,7 @@ static const std::map<std::string, KeyInfo> &dictionary() {
         {"gpu_spmv_tune", {'I', "", "0", "4", ""}},
         {"gpu_level_bf16", {'I', "", "0", "50", ""}},
         {"gpu_seed", {'I', "", "", "", ""}},
-        {"gpu_persistent", {'I', "", "0", "1", ""}},
+        {"gpu_persistent", {'I', "", "0", "16", ""}},
         {"gpu_solve_graph", {'I', "", "0", "1", ""}},
     };
     return d;

@@ -88,7 +88,8 @@ struct SolverCfg {
                                 // 4: no tuning, the x-staged kernel where built)
     int gpu_level_bf16 = 0;     // finest FP32 cycle levels whose matrix values are BF16
     int gpu_seed = 0;           // seed of the host setup's random choices
-    int gpu_persistent = 1;     // eligible BiCGStab solves in one cooperative launch
+    int gpu_persistent = 1;     // eligible BiCGStab solves in one cooperative launch, each
+                                // block playing this many canonical blocks (0: off)
     int gpu_solve_graph = 1;    // whole BiCGStab solves as one graph with a device-side loop
 };
 

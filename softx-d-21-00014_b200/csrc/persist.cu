@@ -5,32 +5,38 @@
 namespace xg {
 namespace ops {
 
-// The whole iteration runs as one cooperative launch of B = canon_blocks(n,
-// nv) blocks (block b is canonical block b), so B blocks must be resident at
-// once, and the two halves of the partial-sum buffer must hold B x nv x 4
-// values each.
+// The whole iteration runs as one cooperative launch: B = canon_blocks(n,
+// nv) canonical blocks played by ceil(B / share) physical blocks (share =
+// gpu_persistent: canonical blocks a physical block plays), which must be
+// resident at once; the two halves of the partial-sum buffer must hold B x
+// nv x 4 values each.
+static int grid_of(int B, int share) { return (B + share - 1) / (share < 1 ? 1 : share); }
+
 template <int NV, typename I>
-static bool fits_nv(uint64_t n) {
+static bool fits_nv(uint64_t n, int share) {
     const int B = k::canon_blocks(n, NV);
     if ((uint64_t)B * NV * 8 > (uint64_t)k::BMAX * 32 * 4) return false;
     const int res = resident_blocks(k::k_pbicgstab_persist<NV, I>, k::CT, 0);
-    return (uint64_t)res * (uint64_t)ctx().sms >= (uint64_t)B;
+    return (uint64_t)res * (uint64_t)ctx().sms >= (uint64_t)grid_of(B, share);
 }
 
-bool pbicgstab_persist_fits(const DCsr &A, int nv) {
+bool pbicgstab_persist_fits(const DCsr &A, int nv, int share) {
     bool ok = false;
-    XG_DISPATCH(A, nv, { ok = fits_nv<NV, I>(A.nrows); });
+    XG_DISPATCH(A, nv, { ok = fits_nv<NV, I>(A.nrows, share); });
     return ok;
 }
 
-void pbicgstab_persist(const DCsr &A, const k::PersistArgs &P, int nv, cudaStream_t s) {
+void pbicgstab_persist(const DCsr &A, const k::PersistArgs &P, int nv, int share,
+                       cudaStream_t s) {
     XG_DISPATCH(A, nv, {
         const int B = k::canon_blocks(A.nrows, NV);
         k::CsrArgs<double> a = A.args<double>();
         k::PersistArgs p = P;
+        p.B = (uint32_t)B;
         void *args[] = {(void *)&a, (void *)&p};
         XG_CUDA(cudaLaunchCooperativeKernel((const void *)k::k_pbicgstab_persist<NV, I>,
-                                            dim3((unsigned)B), dim3(k::CT), args, 0, s));
+                                            dim3((unsigned)grid_of(B, share)), dim3(k::CT), args,
+                                            0, s));
         ++g_kernel_launches;
     });
 }

@@ -1225,17 +1225,16 @@ bool Krylov::started() {
 // gpu_persistent (default 1): the preconditioned forms (PBiCGStab,
 // MergedPBiCGStab) with the Identity (no preconditioner list) or a Jacobi
 // preconditioner without its own convergence test run every iteration in
-// one cooperative launch
-// when the matrix's canonical blocks fit the GPU at once (small and
-// mid-sized systems; the 32^3 Poisson system has 128); printing residuals
-// (convergence_info) keeps the host loop.
+// one cooperative launch when its blocks (the canonical blocks, 128 for the
+// 32^3 Poisson system, shared gpu_persistent to a block) fit the GPU at
+// once; printing residuals (convergence_info) keeps the host loop.
 bool Krylov::persistent_ok() const {
     if (!cfg.gpu_persistent || !precond_form || cfg.convergence_info || f32) return false;
     if (M && !dynamic_cast<const Identity<double> *>(M.get())) {
         auto *j = dynamic_cast<const Jacobi<double> *>(M.get());
         if (!j || j->cfg.convergence_check || j->f32) return false;
     }
-    return ops::pbicgstab_persist_fits(*A, NV);
+    return ops::pbicgstab_persist_fits(*A, NV, cfg.gpu_persistent);
 }
 
 void Krylov::run_persistent(DVec &x) {
@@ -1268,7 +1267,7 @@ void Krylov::run_persistent(DVec &x) {
     P.rel_tol = cfg.rel_tol;
     P.ra = ra;
     P.gs = k::GridSync{psync.as<unsigned>(), psync.as<unsigned>() + 1, ra.flag, 1000000000ull};
-    ops::pbicgstab_persist(*A, P, NV, s);
+    ops::pbicgstab_persist(*A, P, NV, cfg.gpu_persistent, s);
     double out[97];
     XG_CUDA(cudaMemcpyAsync(out, pout.p, sizeof(out), cudaMemcpyDeviceToHost, s));
     ctx().check_flags();  // synchronises; XAMG_ERR_TIMEOUT if a grid wait ran out

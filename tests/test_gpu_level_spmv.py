@@ -187,8 +187,9 @@ def test_x_staged_kernel_bit_exact(gpu, oracle, nv, bf16):
     multigrid levels with long rows): each tile's x rows copied once into
     shared memory by unique column, each row summed from there in entry
     order. Every element equals the oracle's sequential row sum, for y = A x
-    and y += A x, on the FP32 cycle operator (FP32 or BF16 values)."""
-    row, col, val = banded_plus_random(6000, 0, 20, seed=nv + 70)
+    and y += A x, on the FP32 cycle operator (FP32 or BF16 values) of a
+    27-point matrix (8,000 rows, diagonal first)."""
+    row, col, val = gpu.generate_diffusion(27, 20, 20, 20, 1.0, 1.0, nv + 70)
     params = {"solver": {"method": "MergedPBiCGStab", "rel_tolerance": 1e-8, "max_iters": 5,
                          "gpu_index_compress": 2},
               "preconditioner": {"method": "MultiGrid", "mg_max_levels": 2,

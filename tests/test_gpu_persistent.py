@@ -32,17 +32,21 @@ def params(method, prec, persistent, max_iters=1000, sweeps=None, tol=1e-8):
                           ("PBiCGStab", True, 8, 1, (16, 16, 16), 1000),
                           ("PBiCGStab", False, 4, None, (17, 16, 15), 1000),
                           ("MergedPBiCGStab", True, 1, None, (32, 32, 32), 7)])
-def test_persistent_equals_stepwise(gpu, method, prec, nv, sweeps, grid, cap):
+@pytest.mark.parametrize("share", [1, 3, 4])
+def test_persistent_equals_stepwise(gpu, method, prec, nv, sweeps, grid, cap, share):
+    """share (gpu_persistent): canonical blocks each block of the launch plays;
+    the reductions stay per canonical block, so every share gives the same
+    bits as the step-by-step solve."""
     row, col, val = gpu.generate_cube(*grid)
     n = len(row) - 1
     b = np.random.default_rng(nv + grid[0]).uniform(-1, 1, n * nv)
     out = {}
-    for persistent in (0, 1):
+    for persistent in (0, share):
         k0 = gpu.kernel_launches()
         x, st, S = gpu_solve(gpu, row, col, val, nv, params(method, prec, persistent, cap, sweeps),
                              b)
         out[persistent] = (x, st, gpu.kernel_launches() - k0)
-    (x0, s0, l0), (x1, s1, l1) = out[0], out[1]
+    (x0, s0, l0), (x1, s1, l1) = out[0], out[share]
     assert s0["iters"] == s1["iters"]
     assert s0["conv"].tolist() == s1["conv"].tolist()
     assert s0["rel_res"].tobytes() == s1["rel_res"].tobytes()
