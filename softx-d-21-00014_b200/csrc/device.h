@@ -206,26 +206,6 @@ void download_csr(const DCsr &d, uint32_t *row, void *col, void *val);
 // (dz, dy, dx)). Sets the pattern, strides and order.
 bool stencil_layout(const HCsr &h, int &pat, uint32_t &S, uint32_t &S2, bool &diag_first);
 
-// A launch with programmatic stream serialization: the solve path's kernels
-// begin with k::pdl_begin (wait for the predecessor, then release the
-// successor), so a kernel's launch overlaps the end of the one before it in
-// the stream (or graph).
-template <typename... KArgs, typename... Args>
-inline void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
-                       Args &&...args) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = s;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    XG_CUDA(cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...));
-}
-
 template <typename T>
 void upload(DevBuf &b, const std::vector<T> &v, cudaStream_t s) {
     b.alloc(v.size() * sizeof(T));

@@ -51,18 +51,6 @@ __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b);
 __device__ __forceinline__ double dvd(double a, double b) { return __ddiv_rn(a, b); }
 __device__ __forceinline__ float dvd(float a, float b) { return __fdiv_rn(a, b); }
 
-// Programmatic dependent launch: the solve path's kernels are launched with
-// programmatic stream serialization, so a kernel's blocks may be scheduled
-// while its predecessor in the stream finishes. Each kernel first waits for
-// the predecessor's completion and memory (griddepcontrol.wait) and only then
-// lets its own successor launch (launch_dependents): one kernel's launch
-// overlaps the previous one's tail, and no block touches data before its
-// producer is done. Launched without the attribute, both are no-ops.
-__device__ __forceinline__ void pdl_begin() {
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
-
 template <typename T>
 __device__ __forceinline__ T shfl_xor(T v, int off) {
     return __shfl_xor_sync(0xffffffffu, v, off);
@@ -436,7 +424,6 @@ template <typename F, typename FX, typename I, int NV, int VK, int NRED, class E
 __global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
     k_spmv(CsrArgs<F> A, const FX *__restrict__ x, Epi epi, RedArgs ra, uint32_t cap,
            uint32_t nbuf, uint32_t B, uint32_t run = 1) {
-    pdl_begin();
     constexpr int G = NV / VK;
     constexpr int R = CT / NV;
     constexpr int NR = NRED > 0 ? NRED : 1;
@@ -563,7 +550,6 @@ template <int NV>
 constexpr int wide_chunk() { return 512 / NV; }  // entries per warp-chunk
 template <typename F, typename FX, typename I, int NV, class Epi, typename V = F>
 __global__ void __launch_bounds__(WT) k_spmv_wide(CsrArgs<F> A, const FX *__restrict__ x, Epi epi) {
-    pdl_begin();
     constexpr int E = NV >= 32 ? 1 : 32 / NV;  // entries a warp gathers per round
     constexpr int CH = wide_chunk<NV>();
     __shared__ F prod[WT / 32][CH * NV];
@@ -630,7 +616,6 @@ static __global__ void k_tile_max(const uint32_t *__restrict__ row, uint64_t n, 
 // these streaming kernels are bound by the loads in flight.
 template <typename F, int NV, int NRED, class Epi>
 __global__ void __launch_bounds__(CT, 4) k_rows(uint64_t n, Epi epi, RedArgs ra) {
-    pdl_begin();
     constexpr int R = CT / NV;
     const int rt = threadIdx.x / NV, k = threadIdx.x % NV;
     const uint64_t ntiles = (n + R - 1) / R;
@@ -946,7 +931,6 @@ struct EGroup4 {
 // ---------------------------------------------------------------------------
 template <class Op>
 __global__ void __launch_bounds__(CT) k_flat(uint64_t m, Op op) {
-    pdl_begin();
     for (uint64_t e = (uint64_t)blockIdx.x * CT + threadIdx.x; e < m;
          e += (uint64_t)gridDim.x * CT)
         op(e);
@@ -1283,7 +1267,6 @@ __global__ void __launch_bounds__(CT)
                  const F *__restrict__ val, const uint64_t *__restrict__ boff, int nblocks,
                  const F *__restrict__ t, F *__restrict__ x, const F *__restrict__ d,
                  const double *__restrict__ relax_sc) {
-    pdl_begin();
     const uint64_t gt = (uint64_t)blockIdx.x * CT + threadIdx.x;
     const int g = (int)(gt / NV), k = (int)(gt % NV);
     if (g >= nblocks) return;
@@ -1316,7 +1299,6 @@ constexpr int DJ = 64;
 template <typename F, int NV>
 __global__ void __launch_bounds__(DT)
     k_dense(const F *__restrict__ a, uint64_t n, const F *__restrict__ x, F *__restrict__ y) {
-    pdl_begin();
     constexpr int RB = DT / NV;  // rows a block
     __shared__ F xs[DJ * NV];
     __shared__ F as[DJ * RB];

@@ -43,7 +43,6 @@ __device__ static bool loop_converged(double *sc, double *out, const LoopCtl &c,
 // the test against rho0 itself; the loop runs unless that already passes
 // (its first iteration runs whatever max_iters is, as the host loop's does).
 __global__ void k_loop_start(double *sc, double *out, LoopCtl c) {
-    pdl_begin();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     for (int k = 0; k < c.nv; ++k) {
         sc[SC_ICONV * SC_STRIDE + k] = 1.0;
@@ -62,7 +61,6 @@ __global__ void k_loop_start(double *sc, double *out, LoopCtl c) {
 // update (converged); the loop goes on while neither converged nor at
 // max_iters.
 __global__ void k_loop_check(double *sc, double *out, LoopCtl c) {
-    pdl_begin();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     const int it = (int)out[LOOP_ITERS] + 1;
     out[LOOP_ITERS] = (double)it;
@@ -78,13 +76,13 @@ __global__ void k_loop_check(double *sc, double *out, LoopCtl c) {
 namespace ops {
 
 void loop_start(double *sc, double *out, const k::LoopCtl &c, cudaStream_t s) {
-    launch_pdl(k::k_loop_start, dim3(1), dim3(32), 0, s, sc, out, c);
+    k::k_loop_start<<<1, 32, 0, s>>>(sc, out, c);
     XG_CUDA(cudaGetLastError());
     ++g_kernel_launches;
 }
 
 void loop_check(double *sc, double *out, const k::LoopCtl &c, cudaStream_t s) {
-    launch_pdl(k::k_loop_check, dim3(1), dim3(32), 0, s, sc, out, c);
+    k::k_loop_check<<<1, 32, 0, s>>>(sc, out, c);
     XG_CUDA(cudaGetLastError());
     ++g_kernel_launches;
 }

@@ -33,8 +33,9 @@ void hsgs_sweep(const DCsr &A, const uint64_t *boff, int nblocks, const F *t, F 
     XG_DISPATCH(A, nv, {
         const uint64_t threads = (uint64_t)nblocks * NV;
         const int B = (int)((threads + k::CT - 1) / k::CT);
-        launch_pdl(k::k_hsgs_sweep<F, I, NV>, dim3(B), dim3(k::CT), 0, s, A.row.as<uint32_t>(),
-                   (const I *)A.col.p, A.val.as<F>(), boff, nblocks, t, x, d, relax_sc);
+        k::k_hsgs_sweep<F, I, NV><<<B, k::CT, 0, s>>>(A.row.as<uint32_t>(), (const I *)A.col.p,
+                                                      A.val.as<F>(), boff, nblocks, t, x, d,
+                                                      relax_sc);
         XG_CUDA(cudaGetLastError());
         ++g_kernel_launches;
     });
@@ -50,8 +51,7 @@ void dense_apply(const F *a, uint64_t n, const F *x, F *y, int nv, cudaStream_t 
     dispatch_nv(nv, [&](auto nvc) {
         constexpr int NV = decltype(nvc)::value;
         constexpr uint64_t RB = k::DT / NV;
-        launch_pdl(k::k_dense<F, NV>, dim3((unsigned)((n + RB - 1) / RB)), dim3(k::DT), 0, s, a, n,
-                   x, y);
+        k::k_dense<F, NV><<<(unsigned)((n + RB - 1) / RB), k::DT, 0, s>>>(a, n, x, y);
         XG_CUDA(cudaGetLastError());
         ++g_kernel_launches;
     });

@@ -126,7 +126,7 @@ static void flat(uint64_t m, const Op &op, cudaStream_t s) {
     if (m == 0) return;
     uint64_t blocks = (m + k::CT - 1) / k::CT;
     if (blocks > (uint64_t)k::BMAX * 4) blocks = (uint64_t)k::BMAX * 4;
-    launch_pdl(k::k_flat<Op>, dim3((unsigned)blocks), dim3(k::CT), 0, s, m, op);
+    k::k_flat<Op><<<(unsigned)blocks, k::CT, 0, s>>>(m, op);
     XG_CUDA(cudaGetLastError());
     ++g_kernel_launches;
 }

@@ -136,8 +136,8 @@ static void launch_vk(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s
     const uint32_t B = NRED > 0 ? (uint32_t)k::canon_blocks(A.nrows, NV)
                                 : (uint32_t)std::min<uint64_t>((ntiles + run - 1) / run, wave);
     const uint32_t P = (uint32_t)std::min<uint64_t>(B, wave);
-    launch_pdl(kern, dim3(P), dim3(NT), smem, s, A.args<F>(), x, epi, ctx().red(), cap, nbuf, B,
-               run);
+    kern<<<P, NT, smem, s>>>(A.args<F>(), x, epi, ctx().red(), cap, nbuf, B, run);
+    XG_CUDA(cudaGetLastError());
     ++g_kernel_launches;
 }
 
@@ -150,7 +150,8 @@ static void launch_wide(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t
     const int res = resident_blocks(kern, k::WT, 0);
     const uint64_t need = (A.nrows + k::WT / 32 - 1) / (k::WT / 32);
     const uint32_t P = (uint32_t)std::min<uint64_t>(need, (uint64_t)res * ctx().sms);
-    launch_pdl(kern, dim3(P), dim3(k::WT), 0, s, A.args<F>(), x, epi);
+    kern<<<P, k::WT, 0, s>>>(A.args<F>(), x, epi);
+    XG_CUDA(cudaGetLastError());
     ++g_kernel_launches;
 }
 // The x-staged kernel (k_spmv_xs) on a matrix's x-staged copy for NV: one
@@ -175,7 +176,8 @@ static void launch_xs(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s
     const uint32_t P = (uint32_t)std::min<uint64_t>(ntiles, (uint64_t)res * ctx().sms);
     const k::XsArgs xa{A.xs_uptr.as<uint32_t>(), A.xs_ucol.as<uint32_t>(),
                        A.xs_slot.as<uint16_t>(), A.xs_umax, A.xs_emax};
-    launch_pdl(kern, dim3(P), dim3(NT), smem, s, A.args<F>(), xa, x, epi, ctx().red().flag);
+    kern<<<P, NT, smem, s>>>(A.args<F>(), xa, x, epi, ctx().red().flag);
+    XG_CUDA(cudaGetLastError());
     ++g_kernel_launches;
 }
 
@@ -377,8 +379,8 @@ static void launch_stencil_p(const DCsr &A, const F *x, const Epi &epi, cudaStre
     const k::StencilArgs a{A.st_val.p,  A.st_mask.as<uint32_t>(), (uint32_t)A.nrows, A.st_S,
                            A.st_S2,     A.st_SP,                  A.st_slot,
                            A.st_diag_first ? 1 : 0};
-    launch_pdl(kern, dim3(P), dim3(k::ST_THREADS), nbuf * BUF, s, a, x, epi, nbuf,
-               ctx().red().flag);
+    kern<<<P, k::ST_THREADS, nbuf * BUF, s>>>(a, x, epi, nbuf, ctx().red().flag);
+    XG_CUDA(cudaGetLastError());
     ++g_kernel_launches;
 }
 // regs: 0 the 64-register form, 1 the 128-register form
@@ -507,7 +509,8 @@ template <typename F, int NV, int NRED, class Epi>
 static void launch_rows(uint64_t n, const Epi &epi, cudaStream_t s) {
     if (n == 0) return;
     const int B = k::canon_blocks(n, NV);
-    launch_pdl(k::k_rows<F, NV, NRED, Epi>, dim3(B), dim3(k::CT), 0, s, n, epi, ctx().red());
+    k::k_rows<F, NV, NRED, Epi><<<B, k::CT, 0, s>>>(n, epi, ctx().red());
+    XG_CUDA(cudaGetLastError());
     ++g_kernel_launches;
 }
 

@@ -103,7 +103,6 @@ template <typename F, typename FX, int NV, int VK, int M, int PAT, int MINB, cla
 __global__ void __launch_bounds__(ST_THREADS, MINB)
     k_spmv_stencil(StencilArgs A, const FX *__restrict__ x, Epi epi, uint32_t nbuf,
                    unsigned *flag) {
-    pdl_begin();
     constexpr int G = NV / VK;
     constexpr uint32_t TX = st_tx<G>();
     constexpr int K = st_slots<PAT>();

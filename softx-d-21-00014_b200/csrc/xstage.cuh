@@ -78,7 +78,6 @@ __host__ __device__ inline uint32_t xs_smem_bytes(uint32_t umax, uint32_t emax) 
 template <typename F, typename FX, int NV, int VK, class Epi, typename V = F>
 __global__ void __launch_bounds__(CT / VK)
     k_spmv_xs(CsrArgs<F> A, XsArgs X, const FX *__restrict__ x, Epi epi, unsigned *flag) {
-    pdl_begin();
     constexpr int G = NV / VK;
     constexpr int R = CT / NV;
     constexpr int NT = CT / VK;
