@@ -139,8 +139,9 @@ int XAMG_b200_solver_level_info(size_t sid, int level, int which, uint64_t *nrow
  * picked for level matrix `which` (no counterpart): 24 codes, index
  * [value type is float][x type is float][log2 nv]; 0 = not tuned (yet), else
  * 1 + 9 * (right-hand sides a thread: 0 the default of 2 for double and 4 for
- * float x, 1 the other one) + 3 * (staging: 0 one buffer, 1 two, 2 none) +
- * (consecutive tiles a block takes: 0 one, 1 four, 2 sixteen), or 19: one warp per row (its
+ * float x, 1 the other one, 2 eight for float x at nv >= 8) + 3 * (staging: 0 one
+ * buffer, 1 two, 2 none) +
+ * (consecutive tiles a block takes: 0 one, 1 four, 2 sixteen), or 28: one warp per row (its
  * gathers in flight together, products summed in entry order; a candidate for matrices of at
  * most 2^20 rows times nv). Only SpMVs without dot products are tuned; every shape gives the
  * same results bit for bit. */

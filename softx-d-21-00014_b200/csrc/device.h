@@ -139,9 +139,9 @@ struct DCsr {
     // SpMV autotuning (library-owned matrices, gpu_spmv_tune): the launch
     // shape measured fastest for the SpMVs without dot products, per
     // [value type is float][x type is float][log2 nv]: 0 = not tuned yet,
-    // else 1 + 9 * (right-hand sides a thread: 0 default, 1 alternative) +
-    // 3 * (staging: 0 one buffer, 1 two, 2 none) + (tile run: 0 one, 1 four,
-    // 2 sixteen), or 19: the warp-per-row kernel (k_spmv_wide)
+    // else 1 + 9 * (right-hand sides a thread: 0 default, 1 alternative, 2
+    // eight) + 3 * (staging: 0 one buffer, 1 two, 2 none) + (tile run: 0 one,
+    // 1 four, 2 sixteen), or 28: the warp-per-row kernel (k_spmv_wide)
     bool tune_on = false;
     mutable uint8_t tuned[2][2][6] = {};
     // Grid-stencil copy (gpu_index_compress = 3, csrc/stencil.cuh): the slot

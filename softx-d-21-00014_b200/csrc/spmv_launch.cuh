@@ -191,11 +191,12 @@ static bool xs_usable(const DCsr &A, const FX *x) {
            k::xs_smem_bytes<FX, V, NV>(A.xs_umax, A.xs_emax) <= 96u * 1024u;
 }
 
-constexpr uint8_t TUNE_WIDE = 19;         // autotuner code of the warp-per-row kernel
+constexpr uint8_t TUNE_WIDE = 28;         // autotuner code of the warp-per-row kernel
 constexpr uint64_t WIDE_MAX_VALUES = 1u << 20;  // rows * nv up to which it is a candidate
 
 // Autotuner of the SpMVs without dot products: the right-hand sides a thread
-// carries (2 or 4; the alternative of spmv_vk's choice), the staging buffers
+// carries (2 or 4; the alternative of spmv_vk's choice; 8 for FP32 x at
+// nv >= 8), the staging buffers
 // (1, 2, or none: tiles read from global memory, for small matrices where the
 // copy's round trip is not hidden) and the run of consecutive tiles a block
 // takes (1, 4 or 16) are
@@ -214,6 +215,14 @@ inline Tuned tuned_shape(uint8_t code) {
     const int c = code - 1;
     return Tuned{c / 9, (uint32_t)((c / 3) % 3 + 1), TUNE_RUNS[c % 3]};
 }
+// Eight right-hand sides a thread (one thread a row at nv = 8): a third
+// shape the autotuner times for FP32 x and nv >= 8, halving the shared-memory
+// reads of each staged (column, value) pair against four a thread.
+template <typename FX, int NV, int NRED>
+constexpr bool spmv_has_vk8() {
+    return std::is_same<FX, float>::value && NV >= 8 && NRED == 0;
+}
+
 template <typename FX, int NV>
 constexpr int spmv_vk_alt() {
     constexpr int d = k::spmv_vk<FX, NV>();
@@ -235,14 +244,20 @@ static uint8_t autotune(const DCsr &A, const FX *x, cudaStream_t s) {
     XG_CUDA(cudaEventCreate(&e1));
     float best = 1e30f;
     uint8_t code = 1;
-    for (int alt = 0; alt < (VA != VD ? 2 : 1); ++alt)
+    constexpr bool V8 = spmv_has_vk8<FX, NV, 0>() && VD != 8 && VA != 8;
+    for (int alt = 0; alt < 3; ++alt)
         for (uint32_t nb = 1; nb <= 3; ++nb)
             for (int ri = 0; ri < 3; ++ri) {
+                if ((alt == 1 && VA == VD) || (alt == 2 && !V8)) continue;
                 auto go = [&] {
-                    if (alt)
+                    if (alt == 2) {
+                        if constexpr (V8)
+                            launch_vk<F, FX, I, NV, 8, 0, V>(A, x, e, s, nb, TUNE_RUNS[ri]);
+                    } else if (alt) {
                         launch_vk<F, FX, I, NV, VA, 0, V>(A, x, e, s, nb, TUNE_RUNS[ri]);
-                    else
+                    } else {
                         launch_vk<F, FX, I, NV, VD, 0, V>(A, x, e, s, nb, TUNE_RUNS[ri]);
+                    }
                 };
                 // the faster of two rounds of three launches, after one untimed
                 float ms = 1e30f;
@@ -323,6 +338,13 @@ static void launch_v(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s)
             }
             if (t) {
                 const Tuned c = tuned_shape(t);
+                if constexpr (spmv_has_vk8<FX, NV, NRED>() && VK != 8 &&
+                              spmv_vk_alt<FX, NV>() != 8) {
+                    if (c.alt == 2) {
+                        launch_vk<F, FX, I, NV, 8, NRED, V>(A, x, epi, s, c.nbuf, c.run);
+                        return;
+                    }
+                }
                 if (c.alt)
                     launch_vk<F, FX, I, NV, spmv_vk_alt<FX, NV>(), NRED, V>(A, x, epi, s,
                                                                            c.nbuf, c.run);
