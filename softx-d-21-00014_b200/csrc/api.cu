@@ -575,6 +575,11 @@ int XAMG_solver_renew_params(XAMG_param_id pid, XAMG_solver_id sid) {
         keep_gpu(c, sh.root->cfg);
         sh.root->cfg = c;
         Krylov *kr = dynamic_cast<Krylov *>(sh.root.get());
+        // recorded graphs hold the old parameters in their kernels
+        if (kr) {
+            XG_CUDA(cudaStreamSynchronize(ctx().stream));
+            kr->drop_graphs();
+        }
         SolverBase *M = kr ? kr->M.get() : nullptr;
         if (M && Q.has("preconditioner")) {
             SolverCfg pc = resolve_cfg(Q.get("preconditioner"), "preconditioner");

@@ -749,12 +749,7 @@ void Krylov::enable_f32io() {
     sa32.alloc(n, NV, true);
 }
 
-Krylov::~Krylov() {
-    for (auto &kv : graphs_)
-        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
-    for (auto &kv : step_graphs_)
-        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
-}
+Krylov::~Krylov() { drop_graphs(); }
 
 // set_const(out, 0) then precond->solve(out, in) with conv = ones. With
 // gpu_graph (default) the application is recorded once per (out, in,
@@ -1281,6 +1276,18 @@ void Krylov::run_persistent(DVec &x) {
     for (int i = 1; i < 8; ++i) buf[i].zero = false;
     x.zero = false;
     x.init = true;
+}
+
+void Krylov::drop_graphs() {
+    for (auto &kv : graphs_)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    for (auto &kv : step_graphs_)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    for (auto &kv : loop_graphs_)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    graphs_.clear();
+    step_graphs_.clear();
+    loop_graphs_.clear();
 }
 
 // The step graph for key; past 32 keys (many solution vectors) the graphs

@@ -137,6 +137,11 @@ class Krylov : public SolverBase {
     bool loop_ok() const;
     bool launch_loop(DVec &x, DVec &b);
     void loop_done(DVec &x);
+    // Releases every recorded graph (preconditioner applications, iterations,
+    // whole solves): their kernels carry the parameters they were recorded
+    // with, so XAMG_solver_renew_params drops them and they are recorded
+    // again with the new ones.
+    void drop_graphs();
     void begin(DVec &x, DVec &b, const std::vector<double> &conv);
     bool started();
     void step();

@@ -126,3 +126,34 @@ def test_batch_with_loop_graphs(gpu):
             assert st["iters"] == sr["iters"]
             assert st["conv"].tolist() == sr["conv"].tolist()
             assert st["rel_res"].tobytes() == sr["rel_res"].tobytes()
+
+
+def test_renew_params_after_graphs(gpu):
+    """XAMG_solver_renew_params after the solve has been recorded as a graph:
+    the recorded graphs are dropped, and the next solves use the new
+    parameters (here max_iters and the tolerance) as the step-by-step solve
+    does."""
+    row, col, val = gpu.generate_diffusion(27, 14, 13, 12, 1.0, 1.0, 9)
+    n, nv = len(row) - 1, 2
+    b = np.random.default_rng(34).uniform(-1, 1, n * nv)
+    out = {}
+    for loop in (0, 1):
+        M = gpu.Matrix(row, col, val)
+        xv, bv = gpu.Vector(M.n, nv), gpu.Vector(M.n, nv)
+        bv.upload(b)
+        S = gpu.Solver(M, gpu.Params(params("mg32", loop)), xv, bv)
+        for _ in range(4):
+            xv.set(0.0)
+            S.solve()
+        full = S.stats()["iters"]
+        S.renew(gpu.Params({"solver": {"max_iters": 2, "rel_tolerance": 1e-4}},
+                           set_default=False))
+        res = []
+        for _ in range(4):
+            xv.set(0.0)
+            S.solve()
+            st = S.stats()
+            res.append((xv.download().tobytes(), st["iters"], st["rel_res"].tobytes()))
+        out[loop] = (full, res)
+    assert out[0] == out[1]
+    assert out[1][1][-1][1] <= 2 < out[1][0]
