@@ -143,8 +143,12 @@ int XAMG_b200_solver_level_info(size_t sid, int level, int which, uint64_t *nrow
  * buffer, 1 two, 2 none) +
  * (consecutive tiles a block takes: 0 one, 1 four, 2 sixteen), or 28: one warp per row (its
  * gathers in flight together, products summed in entry order; a candidate for matrices of at
- * most 2^20 rows times nv). Only SpMVs without dot products are tuned; every shape gives the
- * same results bit for bit. */
+ * most 2^20 rows times nv), or 29 + 3 * (right-hand sides a thread, as above) + (staging, as
+ * above): the plane walk, where a block takes tiles one grid plane apart in turn so that the x
+ * rows of the planes it gathered last are still in its SM's L1 (a candidate for square
+ * matrices whose rows reach a next plane; gpu_spmv_tune = 5 forces it there without
+ * measuring). Only SpMVs without dot products are tuned; every shape gives the same results
+ * bit for bit. */
 int XAMG_b200_solver_level_tuned(size_t sid, int level, int which, uint8_t *codes);
 
 /* Grid-stencil storage (parameter gpu_index_compress = 3; no counterpart in

@@ -141,9 +141,18 @@ struct DCsr {
     // [value type is float][x type is float][log2 nv]: 0 = not tuned yet,
     // else 1 + 9 * (right-hand sides a thread: 0 default, 1 alternative, 2
     // eight) + 3 * (staging: 0 one buffer, 1 two, 2 none) + (tile run: 0 one,
-    // 1 four, 2 sixteen), or 28: the warp-per-row kernel (k_spmv_wide)
+    // 1 four, 2 sixteen), or 28: the warp-per-row kernel (k_spmv_wide), or
+    // 29 + 3 * (right-hand sides a thread) + (staging): the plane walk
     bool tune_on = false;
     mutable uint8_t tuned[2][2][6] = {};
+    // Plane walk (square matrices with long-range neighbours): walk_rows is
+    // the distance, in rows, from a middle row to the centre of its farthest
+    // neighbour cluster (the next grid plane of a structured grid; 0: none).
+    // A block of the walk takes tiles one such distance apart in turn, so the
+    // x rows of the two planes it gathered last are still in its SM's L1.
+    // walk_force (gpu_spmv_tune = 5): always walk where walk_rows allows.
+    uint32_t walk_rows = 0;
+    bool walk_force = false;
     // Grid-stencil copy (gpu_index_compress = 3, csrc/stencil.cuh): the slot
     // pattern (-1: none, else k::ST_BOX27 or k::ST_STAR7), the line and plane
     // strides, the row order, the per-slot values in the CSR values' type and

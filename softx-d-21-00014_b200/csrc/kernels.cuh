@@ -423,7 +423,7 @@ template <typename F, typename FX, typename I, int NV, int VK, int NRED, class E
           typename V = F>
 __global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
     k_spmv(CsrArgs<F> A, const FX *__restrict__ x, Epi epi, RedArgs ra, uint32_t cap,
-           uint32_t nbuf, uint32_t B, uint32_t run = 1) {
+           uint32_t nbuf, uint32_t B, uint32_t run = 1, uint32_t stride = 0) {
     constexpr int G = NV / VK;
     constexpr int R = CT / NV;
     constexpr int NR = NRED > 0 ? NRED : 1;
@@ -439,7 +439,8 @@ __global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
     const uint64_t n = A.n;
     const uint64_t nnz = n ? row[n] : 0;
     const uint64_t ntiles = (n + R - 1) / R;
-    // tile after t in this physical block's sequence (ntiles: none)
+    // position after t in this physical block's sequence (ntiles: none);
+    // positions are tiles except in the plane walk below
     auto next_tile = [&](uint64_t t) -> uint64_t {
         if constexpr (NRED == 0) {
             if ((t + 1) % run != 0 && t + 1 < ntiles) return t + 1;
@@ -449,6 +450,17 @@ __global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
         if (t + B < ntiles) return t + B;
         const uint64_t c = t % B + gridDim.x;
         return c < B ? c : ntiles;
+    };
+    // Plane walk (no dot products, stride > 0): the blocks run through walk
+    // positions u as above, position u being tile (u % M) * stride + u / M for
+    // u < M * stride (M = ntiles / stride) and tile u after that: a
+    // bijection, under which consecutive positions are tiles stride apart.
+    const uint64_t wM = (NRED == 0 && stride) ? ntiles / stride : 0;
+    const uint64_t wmain = wM * stride;
+    auto tile_at = [&](uint64_t u) -> uint64_t {
+        if constexpr (NRED == 0)
+            if (u < wmain) return (u % wM) * stride + u / wM;
+        return u;
     };
     const uint64_t first = NRED == 0 ? (uint64_t)blockIdx.x * run : (uint64_t)blockIdx.x;
     F acc[VK][NR];
@@ -485,10 +497,12 @@ __global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
         if (vb) bulk_g2s(vdst, vsrc, vb, m);
         if (cb) bulk_g2s(cdst, csrc, cb, m);
     };
-    if (threadIdx.x == 0) issue(first);
+    if (threadIdx.x == 0) issue(tile_at(first));
 
-    for (uint64_t tile = first; tile < ntiles;) {
-        const uint64_t tnext = next_tile(tile);
+    for (uint64_t u = first; u < ntiles;) {
+        const uint64_t unext = next_tile(u);
+        const uint64_t tile = tile_at(u);
+        const uint64_t tnext = unext < ntiles ? tile_at(unext) : ntiles;
         const uint64_t r0 = tile * R;
         const uint64_t r1 = r0 + R < n ? r0 + R : n;
         const uint32_t tj0 = __ldg(&row[r0]), tj1 = __ldg(&row[r1]);
@@ -525,7 +539,7 @@ __global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
         if constexpr (NRED > 0)
             if (tnext == ntiles || tnext % B != tile % B)
                 canon_partial<F, NV, NRED, VK>(acc, ra, (uint32_t)(tile % B));
-        tile = tnext;
+        u = unext;
     }
     if (timed_out) {
         atomicOr(ra.flag, 1u);

@@ -472,6 +472,30 @@ void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s, in
         }
         d.tile_max[l] = mx;
     }
+    // plane-walk distance: of the longest of the 4,096 rows from the middle
+    // on (an interior grid point, where the middle row itself may lie on a
+    // boundary), the midpoint of its forward offsets above half its largest
+    // one (the next plane's 9 entries of a 27-point grid, centred on the
+    // plane offset; the one entry of a 7-point grid)
+    d.walk_rows = 0;
+    d.walk_force = tune == 5;
+    if (h.nrows == h.ncols && h.nrows >= 2) {
+        uint64_t i = h.nrows / 2;
+        for (uint64_t r = i + 1; r < std::min<uint64_t>(h.nrows, h.nrows / 2 + 4096); ++r)
+            if (h.row[r + 1] - h.row[r] > h.row[i + 1] - h.row[i]) i = r;
+        std::vector<uint64_t> off;
+        for (uint64_t j = h.row[i]; j < h.row[i + 1]; ++j)
+            if (h.col[j] > i) off.push_back(h.col[j] - i);
+        if (!off.empty()) {
+            std::sort(off.begin(), off.end());
+            const uint64_t top = off.back();
+            std::vector<uint64_t> far;
+            for (uint64_t o : off)
+                if (2 * o > top) far.push_back(o);
+            const uint64_t w = (far.front() + far.back()) / 2;
+            if (w >= 64 && w <= UINT32_MAX) d.walk_rows = (uint32_t)w;
+        }
+    }
     upload(d.row, h.row, s);
     if (d.col_bytes == -2) {
         std::vector<int16_t> c(h.col.size());

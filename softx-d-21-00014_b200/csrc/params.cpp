@@ -76,7 +76,7 @@ static const std::map<std::string, KeyInfo> &dictionary() {
         {"gpu_index_compress", {'I', "", "0", "3", ""}},
         {"gpu_hsgs_rows", {'I', "", "1", "inf", ""}},
         {"gpu_graph", {'I', "", "0", "1", ""}},
-        {"gpu_spmv_tune", {'I', "", "0", "4", ""}},
+        {"gpu_spmv_tune", {'I', "", "0", "5", ""}},
         {"gpu_level_bf16", {'I', "", "0", "50", ""}},
         {"gpu_seed", {'I', "", "", "", ""}},
         {"gpu_persistent", {'I', "", "0", "16", ""}},

@@ -99,6 +99,18 @@ static int resident_blocks(Kern kern, int threads, size_t smem) {
 // Grid: as many blocks as fit the GPU at once (one wave). With dot products
 // the tiles still go to the canonical B = min(ntiles, 1184) blocks, which the
 // grid's blocks run in turn; without, the grid's blocks take the tiles.
+// run RUN_WALK (no dot products): the plane walk, each block taking one
+// run of consecutive walk positions, the runs as even as the grid allows.
+constexpr uint32_t RUN_WALK = 0xFFFFFFFFu;
+// The plane walk's stride in tiles of R rows (0: the matrix has none, or
+// too few tiles for two planes).
+inline uint32_t walk_stride(const DCsr &A, uint64_t R) {
+    if (!A.walk_rows) return 0;
+    const uint64_t S = (A.walk_rows + R / 2) / R;
+    const uint64_t ntiles = (A.nrows + R - 1) / R;
+    return S >= 2 && ntiles >= 2 * S ? (uint32_t)S : 0u;
+}
+
 template <typename F, typename FX, typename I, int NV, int VK, int NRED, typename V = F,
           class Epi>
 static void launch_vk(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s,
@@ -132,11 +144,16 @@ static void launch_vk(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s
     const uint64_t R = k::CT / NV;
     const uint64_t ntiles = (A.nrows + R - 1) / R;
     const uint64_t wave = (uint64_t)res * (uint64_t)ctx().sms;
+    uint32_t stride = 0;
+    if (NRED == 0 && run == RUN_WALK) {
+        stride = walk_stride(A, R);
+        run = (uint32_t)std::max<uint64_t>(1, (ntiles + wave - 1) / wave);
+    }
     if (NRED > 0 || run < 1) run = 1;
     const uint32_t B = NRED > 0 ? (uint32_t)k::canon_blocks(A.nrows, NV)
                                 : (uint32_t)std::min<uint64_t>((ntiles + run - 1) / run, wave);
     const uint32_t P = (uint32_t)std::min<uint64_t>(B, wave);
-    kern<<<P, NT, smem, s>>>(A.args<F>(), x, epi, ctx().red(), cap, nbuf, B, run);
+    kern<<<P, NT, smem, s>>>(A.args<F>(), x, epi, ctx().red(), cap, nbuf, B, run, stride);
     XG_CUDA(cudaGetLastError());
     ++g_kernel_launches;
 }
@@ -199,7 +216,7 @@ constexpr uint64_t WIDE_MAX_VALUES = 1u << 20;  // rows * nv up to which it is a
 // nv >= 8), the staging buffers
 // (1, 2, or none: tiles read from global memory, for small matrices where the
 // copy's round trip is not hidden) and the run of consecutive tiles a block
-// takes (1, 4 or 16) are
+// takes (1, 4 or 16, or the plane walk where the matrix has a walk stride) are
 // timed with CUDA events on the caller's x into a scratch y (EStore), once
 // per matrix, precision and nv, outside any graph capture; the fastest is
 // kept in the matrix (DCsr::tuned). Matrices of at most WIDE_MAX_VALUES rows
@@ -211,7 +228,12 @@ struct Tuned {
     int alt;
     uint32_t nbuf, run;
 };
+constexpr uint8_t TUNE_WALK0 = 29;  // first code of the plane walk (29..37)
 inline Tuned tuned_shape(uint8_t code) {
+    if (code >= TUNE_WALK0) {
+        const int c = code - TUNE_WALK0;
+        return Tuned{c / 3, (uint32_t)(c % 3 + 1), RUN_WALK};
+    }
     const int c = code - 1;
     return Tuned{c / 9, (uint32_t)((c / 3) % 3 + 1), TUNE_RUNS[c % 3]};
 }
@@ -245,18 +267,20 @@ static uint8_t autotune(const DCsr &A, const FX *x, cudaStream_t s) {
     float best = 1e30f;
     uint8_t code = 1;
     constexpr bool V8 = spmv_has_vk8<FX, NV, 0>() && VD != 8 && VA != 8;
+    // run index 3: the plane walk, where the matrix has one at this nv
+    const int nruns = walk_stride(A, (uint64_t)(k::CT / NV)) ? 4 : 3;
     for (int alt = 0; alt < 3; ++alt)
         for (uint32_t nb = 1; nb <= 3; ++nb)
-            for (int ri = 0; ri < 3; ++ri) {
+            for (int ri = 0; ri < nruns; ++ri) {
                 if ((alt == 1 && VA == VD) || (alt == 2 && !V8)) continue;
+                const uint32_t run = ri == 3 ? RUN_WALK : TUNE_RUNS[ri];
                 auto go = [&] {
                     if (alt == 2) {
-                        if constexpr (V8)
-                            launch_vk<F, FX, I, NV, 8, 0, V>(A, x, e, s, nb, TUNE_RUNS[ri]);
+                        if constexpr (V8) launch_vk<F, FX, I, NV, 8, 0, V>(A, x, e, s, nb, run);
                     } else if (alt) {
-                        launch_vk<F, FX, I, NV, VA, 0, V>(A, x, e, s, nb, TUNE_RUNS[ri]);
+                        launch_vk<F, FX, I, NV, VA, 0, V>(A, x, e, s, nb, run);
                     } else {
-                        launch_vk<F, FX, I, NV, VD, 0, V>(A, x, e, s, nb, TUNE_RUNS[ri]);
+                        launch_vk<F, FX, I, NV, VD, 0, V>(A, x, e, s, nb, run);
                     }
                 };
                 // the faster of two rounds of three launches, after one untimed
@@ -273,7 +297,8 @@ static uint8_t autotune(const DCsr &A, const FX *x, cudaStream_t s) {
                 }
                 if (ms < best) {
                     best = ms;
-                    code = (uint8_t)(1 + alt * 9 + (nb - 1) * 3 + ri);
+                    code = ri == 3 ? (uint8_t)(TUNE_WALK0 + alt * 3 + (nb - 1))
+                                   : (uint8_t)(1 + alt * 9 + (nb - 1) * 3 + ri);
                 }
             }
     if (A.nrows * (uint64_t)NV <= WIDE_MAX_VALUES) {
@@ -323,6 +348,11 @@ static void launch_v(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s)
         }
         if (A.xs_force && xs_usable<FX, V, NV>(A, x)) {
             launch_xs<F, FX, NV, V>(A, x, epi, s);
+            return;
+        }
+        if (A.walk_force && walk_stride(A, (uint64_t)(k::CT / NV)) &&
+            (VK == 1 || (uintptr_t)x % (VK * sizeof(FX)) == 0)) {
+            launch_vk<F, FX, I, NV, VK, NRED, V>(A, x, epi, s, 0, RUN_WALK);
             return;
         }
     }

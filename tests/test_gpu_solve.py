@@ -358,6 +358,39 @@ def test_autotuned_spmv_same_results(gpu, stencil, edge, nv, f32):
     assert out[0][1]["iters"] == out[1][1]["iters"]
 
 
+@pytest.mark.parametrize("stencil,edge,nv,f32", [(27, 20, 8, True), (27, 18, 4, False),
+                                                 (7, 22, 16, True), (27, 17, 2, False)])
+def test_plane_walk_spmv_same_results(gpu, oracle, stencil, edge, nv, f32):
+    """gpu_spmv_tune = 5 runs every SpMV without dot products on a matrix
+    with a plane-walk distance in the walk order (each block taking tiles one
+    grid plane apart; the grids leave tiles past the last whole plane, which
+    keep their order). Only the order in which tiles are visited changes, so
+    the solve equals the untuned one and the oracle in the kernels' order bit
+    for bit."""
+    row, col, val = gpu.generate_diffusion(stencil, edge, edge, edge, 1.0, 1.0, 5)
+    n = len(row) - 1
+    b = np.random.default_rng(10).uniform(-1, 1, n * nv)
+    sm = {"method": "Chebyshev", "polynomial_order": 2}
+    out = {}
+    for tune in (0, 5):
+        params = {"solver": {"method": "MergedPBiCGStab", "max_iters": 100,
+                             "rel_tolerance": 1e-8, "abs_tolerance": 0, "gpu_spmv_tune": tune},
+                  "preconditioner": dict(MG_BASE, method="MultiGrid",
+                                         gpu_precond_f32=1 if f32 else 0, gpu_spmv_tune=tune),
+                  "pre_smoother": sm, "post_smoother": dict(sm),
+                  "coarse_grid_solver": {"method": "Direct"}}
+        if f32:
+            params["solver"]["gpu_index_compress"] = 2
+            params["preconditioner"]["gpu_index_compress"] = 2
+        out[tune] = gpu_solve(gpu, row, col, val, nv, params, b)
+    x5, s5, S5 = out[5]
+    assert out[0][0].tobytes() == x5.tobytes()
+    assert out[0][1]["iters"] == s5["iters"]
+    xo, so, _ = oracle_solve(oracle, S5, row, col, val, nv, params, b, 1)
+    assert s5["iters"] == so["iters"]
+    assert x5.tobytes() == xo.tobytes()
+
+
 @pytest.mark.parametrize("method", ["PCG", "MergedRBiCGStab"])
 def test_graph_fallback_keeps_zero_flag(gpu, method):
     """A preconditioner that reads back its residual (Jacobi with
