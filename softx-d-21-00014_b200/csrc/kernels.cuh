@@ -1337,14 +1337,19 @@ __global__ void __launch_bounds__(DT)
 
 // --- persistent preconditioned BiCGStab ----------------------------------------
 // Grid barrier with a bounded wait: every block of a cooperative launch
-// arrives; the last one opens the next round. A block whose wait passes
-// limit_ns raises the timeout flag (read by the host as XAMG_ERR_TIMEOUT)
-// and returns false, and the kernel then ends; the other blocks' next waits
-// run out the same way, so no block waits without bound.
+// arrives on one 64-bit counter (zero at the launch's start; round r ends when
+// it reaches (r + 1) * expected). Thread 0 of a block arrives with a
+// release-ordered atomic add and polls the counter with acquire-ordered loads;
+// __syncthreads() on both sides extends that ordering to the whole block (the
+// writes of every thread before the barrier are visible to every thread of
+// every block after it). A monotonic counter needs no reset by the last
+// arriver, so the round ends with its own arrival. A block whose wait passes
+// limit_ns raises the timeout flag (read by the host as XAMG_ERR_TIMEOUT) and
+// returns false, and the kernel then ends; the other blocks' next waits run
+// out the same way, so no block waits without bound.
 struct GridSync {
-    unsigned *count;  // arrivals in the current round (zero between rounds)
-    unsigned *gen;    // rounds completed
-    unsigned *flag;   // bit 0: a wait ran out
+    unsigned long long *arrivals;  // zero at the launch's start
+    unsigned *flag;                // bit 0: a wait ran out
     uint64_t limit_ns;
 };
 __device__ __forceinline__ bool grid_sync(const GridSync &g, unsigned expected) {
@@ -1352,24 +1357,31 @@ __device__ __forceinline__ bool grid_sync(const GridSync &g, unsigned expected) 
     __syncthreads();
     if (threadIdx.x == 0) {
         ok = 1;
-        const unsigned round = *(volatile unsigned *)g.gen;
-        __threadfence();
-        if (atomicAdd(g.count, 1u) == expected - 1) {
-            *(volatile unsigned *)g.count = 0u;
-            __threadfence();
-            atomicAdd(g.gen, 1u);
-        } else {
-            const uint64_t t0 = global_ns();
-            for (uint32_t it = 0; *(volatile unsigned *)g.gen == round; ++it) {
-                if (global_ns() - t0 > g.limit_ns || it == 0xffffffffu) {
+        unsigned long long old;
+        asm volatile("atom.add.release.gpu.global.u64 %0, [%1], 1;"
+                     : "=l"(old)
+                     : "l"(g.arrivals)
+                     : "memory");
+        const unsigned long long target = (old / expected + 1ull) * expected;
+        uint64_t t0 = 0;
+        for (uint32_t it = 0;; ++it) {
+            unsigned long long cur;
+            asm volatile("ld.acquire.gpu.global.u64 %0, [%1];"
+                         : "=l"(cur)
+                         : "l"(g.arrivals)
+                         : "memory");
+            if (cur >= target) break;
+            if ((it & 63u) == 0) {  // the clock is read every 64 polls
+                const uint64_t t = global_ns();
+                if (it == 0) {
+                    t0 = t;
+                } else if (t - t0 > g.limit_ns || it >= 0xffffff00u) {
                     atomicOr(g.flag, 1u);
                     ok = 0;
                     break;
                 }
-                __nanosleep(32);
             }
         }
-        __threadfence();
     }
     __syncthreads();
     return ok != 0;

@@ -43,7 +43,7 @@ void pbicgstab_persist(const DCsr &A, const k::PersistArgs &P, int nv, int share
 
 void grid_selftest(unsigned *count_gen, unsigned *flag, uint64_t limit_ns, cudaStream_t s) {
     XG_CUDA(cudaMemsetAsync(count_gen, 0, 2 * sizeof(unsigned), s));
-    k::GridSync g{count_gen, count_gen + 1, flag, limit_ns};
+    k::GridSync g{reinterpret_cast<unsigned long long *>(count_gen), flag, limit_ns};
     const int blocks = 4;  // resident together on any GPU this library runs on
     void *args[] = {(void *)&g};
     XG_CUDA(cudaLaunchCooperativeKernel((const void *)k::k_grid_selftest, dim3(blocks), dim3(32),

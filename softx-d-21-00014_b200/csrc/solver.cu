@@ -1261,7 +1261,7 @@ void Krylov::run_persistent(DVec &x) {
     P.abs_tol = cfg.abs_tol;
     P.rel_tol = cfg.rel_tol;
     P.ra = ra;
-    P.gs = k::GridSync{psync.as<unsigned>(), psync.as<unsigned>() + 1, ra.flag, 1000000000ull};
+    P.gs = k::GridSync{psync.as<unsigned long long>(), ra.flag, 1000000000ull};
     ops::pbicgstab_persist(*A, P, NV, cfg.gpu_persistent, s);
     double out[97];
     XG_CUDA(cudaMemcpyAsync(out, pout.p, sizeof(out), cudaMemcpyDeviceToHost, s));
