@@ -311,7 +311,8 @@ def roofline(X, torch, stream, S, n, nv, args, which=3, reps=50):
     and y written once (x's reuse across rows is served by the caches)."""
     A0 = S.level_csr(0, which)
     esz = 4 if A0.val_f32 else 8                    # x and y elements
-    vsz = {0: 8, 1: 4, 2: 2}[A0.val_f32]             # stored values (2: BF16)
+    vsz = {0: 8, 1: 4, 2: 2, 3: 2}[A0.val_f32]       # stored values (2: BF16, 3: FP16)
+    vname = {2: ", BF16 values", 3: ", FP16 values"}.get(A0.val_f32, "")
     # a grid-stencil copy (gpu_index_compress = 3) is what the SpMV reads:
     # one value per slot and row, a 4-byte entry mask per row, no columns
     st_pat = S.level_stencil(0, which)[0]
@@ -334,12 +335,12 @@ def roofline(X, torch, stream, S, n, nv, args, which=3, reps=50):
         slots = 27 if st_pat == 0 else 7
         alg = slots * n * vsz + n * 4 + 2 * n * nv * esz
         kname = f"k_spmv_stencil<{fname}> level 0, EStore, nv={nv}, " \
-                f"{slots}-slot grid stencil" + (", BF16 values" if vsz == 2 else "")
+                f"{slots}-slot grid stencil" + vname
         tkey = f"{args.workload}_n{n}_which{which}_nv{nv}_v{vsz}_st{slots}"
     else:
         alg = A0.nnz * (vsz + abs(A0.col_bytes)) + (n + 1) * 4 + 2 * n * nv * esz
         kname = f"k_spmv<{fname}> level 0, EStore, nv={nv}, " \
-                f"col_bytes={A0.col_bytes}" + (", BF16 values" if vsz == 2 else "")
+                f"col_bytes={A0.col_bytes}" + vname
         tkey = f"{args.workload}_n{n}_which{which}_nv{nv}_v{vsz}"
     achieved = alg / (ms * 1e-3) / 1e9
     peak, peak_kind = peaks()

@@ -46,7 +46,13 @@ int XAMG_b200_build_info(char *buf, size_t len);
  * lie within 32767 of the diagonal (parameter gpu_index_compress = 2).
  * Row pointers are 32-bit. Values are double (val_f32 = 0), float (1), or
  * BF16 with float arithmetic (2: the FP32 cycle levels that parameter
- * gpu_level_bf16 selects; no counterpart in the reference). */
+ * gpu_level_bf16 selects; no counterpart in the reference). Level matrices
+ * may also report 3: FP16 values with float arithmetic, each stored divided
+ * by the level's power-of-two scale (parameter gpu_level_fp16 = 1 with
+ * gpu_level_bf16 = L; no counterpart in the reference). A descriptor of
+ * form 3 carries no scale and is not accepted as input;
+ * XAMG_b200_solver_level_download returns its values widened to float with
+ * the scale applied. */
 typedef struct {
     uint64_t nrows, ncols, nnz;
     const uint32_t *row;
@@ -177,7 +183,9 @@ int XAMG_b200_solver_level_stencil(size_t sid, int level, int which, int *patter
                                    uint32_t *S2, int *diag_first);
 
 /* Copy level matrix `which` back from the device exactly as stored: row
- * pointers (u32), narrowed columns (col_bytes each), values (float/double). */
+ * pointers (u32), narrowed columns (col_bytes each), values (float/double;
+ * BF16 bits for val_f32 = 2; for val_f32 = 3 the FP16 values widened to
+ * float with the level's scale applied, 4 bytes each). */
 int XAMG_b200_solver_level_download(size_t sid, int level, int which, uint32_t *row, void *col,
                                     void *val);
 

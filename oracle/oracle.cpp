@@ -823,6 +823,26 @@ static Csr to_bf16_values(const Csr &a) {
     return b;
 }
 
+// B200 extension gpu_level_fp16 = 1: the same levels store FP16 values
+// instead, each float value divided by the level's power-of-two scale s
+// (2^(E - 15) for the largest magnitude m * 2^E, m in [0.5, 1); 1 for an
+// all-zero level), rounded to the nearest FP16 (ties to even, IEEE
+// binary16 through the compiler's _Float16) and read back as h * s; the
+// division and the product by s are exact.
+static Csr to_fp16_values(const Csr &a) {
+    Csr b = a;
+    float mx = 0.0f;
+    for (float v : b.vf) mx = std::max(mx, std::fabs(v));
+    float s = 1.0f;
+    if (mx > 0.0f && std::isfinite(mx)) {
+        int E = 0;
+        std::frexp(mx, &E);
+        s = std::ldexp(1.0f, E - 15);
+    }
+    for (float &v : b.vf) v = (float)(_Float16)(v / s) * s;
+    return b;
+}
+
 // csr_matrix.inl:86-170
 static void compress(Csr &m) {
     if (m.empty()) return;
@@ -2091,9 +2111,12 @@ static int setup(System &sys) {
     const std::string mg_role = mg_solver ? "solver" : "preconditioner";
     bool reduced = false, full32 = false;
     int bf16_levels = 0;
+    bool fp16 = false;
     if (mg_solver || mg_prec) {
         std::string bf = sys.P.get(mg_role, "gpu_level_bf16");
         if (!bf.empty()) bf16_levels = (int)std::stol(bf);
+        std::string hf = sys.P.get(mg_role, "gpu_level_fp16");
+        fp16 = !hf.empty() && std::stol(hf) == 1;
         std::string v = sys.P.get(mg_role, "mg_reduced_precision");
         reduced = !v.empty() && std::stol(v) != 0;
         // B200 extension: gpu_precond_f32 = 1 puts the finest level of the
@@ -2115,7 +2138,7 @@ static int setup(System &sys) {
         // gpu_level_bf16: the finest float cycle operators store BF16 values
         // (the smoothers' diagonals and the transfers keep the float values)
         lv.bf16 = lv.reduced && (int)l < bf16_levels;
-        if (lv.bf16) lv.Abf = to_bf16_values(lv.A);
+        if (lv.bf16) lv.Abf = fp16 ? to_fp16_values(lv.A) : to_bf16_values(lv.A);
         lv.min_eig = sys.min_eig[l];
         lv.max_eig = sys.max_eig[l];
         if (l + 1 < L) {

@@ -872,7 +872,7 @@ int XAMG_b200_solver_level_info(size_t sid, int level, int which, uint64_t *nrow
         if (ncols) *ncols = d.ncols;
         if (nnz) *nnz = d.nnz;
         if (col_bytes) *col_bytes = d.col_bytes;
-        if (val_f32) *val_f32 = d.bf16 ? 2 : d.f32 ? 1 : 0;
+        if (val_f32) *val_f32 = d.fp16 ? 3 : d.bf16 ? 2 : d.f32 ? 1 : 0;
         if (hash) *hash = d.hash;
         MultiGrid *mg = solver_mg(sid);
         if (min_eig) *min_eig = mg ? mg->L[level].min_eig : 0.0;
@@ -968,7 +968,7 @@ int XAMG_b200_solver_level_csr(size_t sid, int level, int which, XAMG_b200_csr *
         out->col = d.col.p;
         out->val = d.val.p;
         out->col_bytes = d.col_bytes;
-        out->val_f32 = d.bf16 ? 2 : d.f32 ? 1 : 0;
+        out->val_f32 = d.fp16 ? 3 : d.bf16 ? 2 : d.f32 ? 1 : 0;
     });
 }
 

@@ -131,6 +131,10 @@ struct DCsr {
     int col_bytes = 4;
     bool f32 = false;
     bool bf16 = false;  // float matrix whose values are stored in BF16
+    // float matrix whose values are stored in FP16 divided by vscale, a power
+    // of two that puts the largest magnitude in [2^14, 2^15)
+    bool fp16 = false;
+    float vscale = 1.0f;
     uint16_t hash = 0;
     DevBuf row, col, val;
     // largest number of entries in one tile of 256/nv rows, per nv = 1..32
@@ -180,7 +184,7 @@ struct DCsr {
 
     template <typename F>
     k::CsrArgs<F> args() const {
-        return k::CsrArgs<F>{row.as<uint32_t>(), col.p, val.as<F>(), nrows};
+        return k::CsrArgs<F>{row.as<uint32_t>(), col.p, val.as<F>(), nrows, vscale};
     }
     bool empty() const { return nnz == 0; }
 };
@@ -200,11 +204,15 @@ struct DCsr {
 // warp-per-row kernel.
 // bf16 (with f32): store the values rounded to float and then to BF16
 // (round to nearest even), the arithmetic staying in float.
+// fp16 (with f32, instead of bf16): store each value rounded to float,
+// divided by the matrix's power-of-two scale (exact) and rounded to FP16
+// (nearest even); the SpMVs read h * scale (exact). No grid-stencil or
+// x-staged copy is built for such a matrix.
 // xs_nv (narrow >= 2, tune = 4): also build the x-staged copy for SpMVs with
 // xs_nv right-hand sides, where the rows are long enough and a tile's x rows
 // fit in shared memory.
 void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s, int tune = 0,
-                bool bf16 = false, int xs_nv = 0);
+                bool bf16 = false, int xs_nv = 0, bool fp16 = false);
 void download_csr(const DCsr &d, uint32_t *row, void *col, void *val);
 
 // Whether a square CSR block has the grid-stencil structure of

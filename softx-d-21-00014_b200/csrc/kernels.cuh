@@ -28,6 +28,7 @@
 #pragma once
 
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -198,6 +199,7 @@ struct CsrArgs {
     const void *col;
     const F *val;
     uint64_t n;
+    float vscale = 1.0f;  // FP16-stored values: the level's power-of-two scale
 };
 
 // Shared-memory staging: a tile's entries [row[r0], row[r0+R]) (values and
@@ -288,6 +290,15 @@ __device__ __forceinline__ F val_as(V v) {
     else
         return (F)v;
 }
+// The same with a scale: an FP16-stored value times its level's power-of-two
+// scale (an exact product), every other storage type as above.
+template <typename F, typename V>
+__device__ __forceinline__ F val_as(V v, float sc) {
+    if constexpr (std::is_same<V, __half>::value)
+        return (F)__fmul_rn(__half2float(v), sc);
+    else
+        return val_as<F, V>(v);
+}
 
 // Column index in 32 bits (the launcher checks that every x offset c*NV + k
 // fits): the gather address is one 32-bit multiply-add and one widening add.
@@ -301,12 +312,12 @@ __device__ __forceinline__ uint32_t col_at32(I c, uint32_t i) {
 
 template <typename F, typename FX, typename I, int NV, int VK, typename V = F>
 __device__ __forceinline__ void row_sum(F (&y)[VK], uint32_t len, uint64_t i, int k0, const I *cl,
-                                        const V *vl, const FX *x) {
+                                        const V *vl, const FX *x, float vsc = 1.0f) {
     const uint32_t i32 = (uint32_t)i;
 #pragma unroll SPMV_UNROLL
     for (uint32_t j = 0; j < len; ++j) {
         const uint32_t c = col_at32<I>(cl[j], i32);
-        const F av = val_as<F, V>(vl[j]);
+        const F av = val_as<F, V>(vl[j], vsc);
         FX xv[VK];
         ld_x<FX, VK>(x + (c * (uint32_t)NV + (uint32_t)k0), xv);
 #pragma unroll
@@ -528,9 +539,9 @@ __global__ void __launch_bounds__(CT / VK, spmv_min_blocks<VK>())
             const uint32_t j0 = __ldg(&row[i]), j1 = __ldg(&row[i + 1]);
             if (staged)
                 row_sum<F, FX, I, NV, VK, V>(y, j1 - j0, i, k0, sc + (j0 - tj0), sv + (j0 - tj0),
-                                             x);
+                                             x, A.vscale);
             else
-                row_sum<F, FX, I, NV, VK, V>(y, j1 - j0, i, k0, col + j0, val + j0, x);
+                row_sum<F, FX, I, NV, VK, V>(y, j1 - j0, i, k0, col + j0, val + j0, x, A.vscale);
 #pragma unroll
             for (int v = 0; v < VK; ++v) epi.store(i, k0 + v, y[v], acc[v]);
         }
@@ -583,7 +594,7 @@ __global__ void __launch_bounds__(WT) k_spmv_wide(CsrArgs<F> A, const FX *__rest
 #pragma unroll 4
             for (uint32_t e = es; e < len; e += E) {
                 const uint32_t c = col_at32<I>(__ldg(&col[c0 + e]), i32);
-                const F av = val_as<F, V>(__ldg(&val[c0 + e]));
+                const F av = val_as<F, V>(__ldg(&val[c0 + e]), A.vscale);
                 pw[e * NV + k] = mul((F)__ldg(&x[c * (uint32_t)NV + (uint32_t)k]), av);
             }
             __syncwarp();

@@ -78,6 +78,7 @@ static const std::map<std::string, KeyInfo> &dictionary() {
         {"gpu_graph", {'I', "", "0", "1", ""}},
         {"gpu_spmv_tune", {'I', "", "0", "5", ""}},
         {"gpu_level_bf16", {'I', "", "0", "50", ""}},
+        {"gpu_level_fp16", {'I', "", "0", "1", ""}},
         {"gpu_seed", {'I', "", "", "", ""}},
         {"gpu_persistent", {'I', "", "0", "16", ""}},
         {"gpu_solve_graph", {'I', "", "0", "1", ""}},
@@ -358,6 +359,7 @@ SolverCfg resolve_cfg(const PList &l, const std::string &role) {
     c.gpu_graph = l.get_i("gpu_graph", 1);
     c.gpu_spmv_tune = l.get_i("gpu_spmv_tune", 1);
     c.gpu_level_bf16 = l.get_i("gpu_level_bf16", 0);
+    c.gpu_level_fp16 = l.get_i("gpu_level_fp16", 0);
     c.gpu_seed = l.get_i("gpu_seed", 0);
     c.gpu_persistent = l.get_i("gpu_persistent", 1);
     c.gpu_solve_graph = l.get_i("gpu_solve_graph", 1);

@@ -85,8 +85,11 @@ struct SolverCfg {
     int gpu_spmv_tune = 1;      // SpMV launch shapes picked by measurement (2: no tuning,
                                 // the grid-stencil kernel's 128-register form; 3: no
                                 // tuning, the warp-per-row kernel on small matrices;
-                                // 4: no tuning, the x-staged kernel where built)
+                                // 4: no tuning, the x-staged kernel where built; 5: no
+                                // tuning, the plane walk where the matrix has one)
     int gpu_level_bf16 = 0;     // finest FP32 cycle levels whose matrix values are BF16
+    int gpu_level_fp16 = 0;     // 1: those levels store FP16 values with a per-level
+                                // power-of-two scale instead of BF16
     int gpu_seed = 0;           // seed of the host setup's random choices
     int gpu_persistent = 1;     // eligible BiCGStab solves in one cooperative launch, each
                                 // block playing this many canonical blocks (0: off)

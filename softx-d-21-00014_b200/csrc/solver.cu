@@ -525,10 +525,14 @@ void MultiGrid::build(const HCsr &A0, const DCsr *A0dev, const Params &P, const 
         lv.min_eig = HH.lv[l].min_eig;
         lv.max_eig = HH.lv[l].max_eig;
         // gpu_level_bf16: the l < gpu_level_bf16 finest FP32 cycle operators store
-        // BF16 values (the smoothers' diagonals stay float from the exact values)
-        if (l >= 1 || full32)
+        // BF16 values, or with gpu_level_fp16 = 1 FP16 values with a per-level
+        // power-of-two scale (the smoothers' diagonals stay float from the
+        // exact values)
+        if (l >= 1 || full32) {
+            const bool half = lv.f32 && l < cfg.gpu_level_bf16;
             upload_csr(HH.lv[l].A, lv.A, lv.f32, narrow, S(), tune,
-                       lv.f32 && l < cfg.gpu_level_bf16, nv);
+                       half && cfg.gpu_level_fp16 == 0, nv, half && cfg.gpu_level_fp16 == 1);
+        }
         if (l + 1 < nl) {
             // R = P^T (hypre_base.inl:400-401, transpose.inl:31-108)
             const HCsr &Ph = HH.lv[l].P;

@@ -346,10 +346,11 @@ static void launch_v(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s)
             launch_wide<F, FX, I, NV, V>(A, x, epi, s);
             return;
         }
-        if (A.xs_force && xs_usable<FX, V, NV>(A, x)) {
-            launch_xs<F, FX, NV, V>(A, x, epi, s);
-            return;
-        }
+        if constexpr (!std::is_same<V, __half>::value)
+            if (A.xs_force && xs_usable<FX, V, NV>(A, x)) {
+                launch_xs<F, FX, NV, V>(A, x, epi, s);
+                return;
+            }
         if (A.walk_force && walk_stride(A, (uint64_t)(k::CT / NV)) &&
             (VK == 1 || (uintptr_t)x % (VK * sizeof(FX)) == 0)) {
             launch_vk<F, FX, I, NV, VK, NRED, V>(A, x, epi, s, 0, RUN_WALK);
@@ -551,9 +552,13 @@ static void launch(const DCsr &A, const FX *x, const Epi &epi, cudaStream_t s) {
             launch_v<F, FX, I, NV, NRED, CALLER_X, __nv_bfloat16>(A, x, epi, s);
             return;
         }
+        if (A.fp16) {
+            launch_v<F, FX, I, NV, NRED, CALLER_X, __half>(A, x, epi, s);
+            return;
+        }
     }
-    XG_REQUIRE(!A.bf16, XAMG_ERR_UNSUPPORTED,
-               "BF16 matrix values need float values and a float x");
+    XG_REQUIRE(!A.bf16 && !A.fp16, XAMG_ERR_UNSUPPORTED,
+               "16-bit matrix values need float values and a float x");
     launch_v<F, FX, I, NV, NRED, CALLER_X, F>(A, x, epi, s);
 }
 

@@ -328,7 +328,7 @@ class Params:
                 "mg_agg_interpolation_type", "mg_agg_Pmax_elements", "mg_agg_P12max_elements",
                 "gpu_precond_f32", "gpu_coarse_f64", "gpu_index_compress", "gpu_hsgs_rows",
                 "gpu_graph", "gpu_seed", "gpu_persistent", "gpu_spmv_tune", "gpu_level_bf16",
-                "gpu_solve_graph"}
+                "gpu_level_fp16", "gpu_solve_graph"}
 
     def __init__(self, spec=None, overrides=None, set_default=True):
         h = sz()
@@ -526,7 +526,7 @@ class Solver:
         call("XAMG_b200_solver_level_info", self.h, level, which, C.byref(nr), C.byref(nc),
              C.byref(nz), C.byref(cb), C.byref(f32), C.byref(hsh), C.byref(mn), C.byref(mx))
         return dict(nrows=nr.value, ncols=nc.value, nnz=nz.value, col_bytes=cb.value,
-                    f32=bool(f32.value), bf16=f32.value == 2, hash=hsh.value, min_eig=mn.value,
+                    f32=bool(f32.value), bf16=f32.value == 2, fp16=f32.value == 3, hash=hsh.value, min_eig=mn.value,
                     max_eig=mx.value)
 
     def level_tuned(self, level, which):
@@ -557,7 +557,7 @@ class Solver:
                                      -2: np.int16}[info["col_bytes"]])
         if info["bf16"]:  # BF16 bits, widened to float32 below
             val = np.zeros(info["nnz"], np.uint16)
-        else:
+        else:  # FP16 values come back widened to float32, their scale applied
             val = np.zeros(info["nnz"], np.float32 if info["f32"] else np.float64)
         call("XAMG_b200_solver_level_download", self.h, level, which, _ptr(row), _ptr(col),
              _ptr(val))

@@ -48,11 +48,14 @@ def test_config5_anisotropic_27pt_vcycle22_cheby3(gpu, oracle):
     assert st["iters"] < 80
 
 
-@pytest.mark.parametrize("levels,smoother", [(1, "Chebyshev"), (2, "Chebyshev"),
-                                              (2, "Jacobi"), (2, "HSGS")])
-def test_config5_bf16_levels(gpu, oracle, levels, smoother):
-    """Configuration 5's BF16 level values (gpu_level_bf16: the finest FP32
-    cycle operators store BF16 values, float arithmetic; smoother diagonals,
+@pytest.mark.parametrize("levels,smoother,half", [(1, "Chebyshev", "bf16"),
+                                                   (2, "Chebyshev", "bf16"), (2, "Jacobi", "bf16"),
+                                                   (2, "HSGS", "bf16"), (2, "Chebyshev", "fp16"),
+                                                   (2, "HSGS", "fp16")])
+def test_config5_bf16_levels(gpu, oracle, levels, smoother, half):
+    """Configuration 5's 16-bit level values (gpu_level_bf16: the finest FP32
+    cycle operators store BF16 values, or with gpu_level_fp16 = 1 FP16 values
+    scaled by a per-level power of two; float arithmetic; smoother diagonals,
     hybrid Gauss-Seidel blocks and transfers from the float values). The
     oracle given the same setup replays the solve bit for bit, XAMG's order
     agrees to 1e-6, and the true residuals reach the tolerance."""
@@ -67,8 +70,9 @@ def test_config5_bf16_levels(gpu, oracle, levels, smoother):
     params = {"solver": {"method": "MergedPBiCGStab", "max_iters": 200, "rel_tolerance": 1e-8,
                          "abs_tolerance": 0, "gpu_index_compress": 2},
               "preconditioner": dict(MG_BASE, method="MultiGrid", gpu_precond_f32=1,
-                                     gpu_index_compress=2, gpu_level_bf16=levels),
+                                     gpu_index_compress=2, gpu_level_bf16=levels,
+                                     gpu_level_fp16=1 if half == "fp16" else 0),
               "pre_smoother": sm, "post_smoother": dict(sm),
               "coarse_grid_solver": {"method": "Direct"}}
     st, S = check(gpu, oracle, row, col, val, nv, params, seed=5, tol=1.5e-9)
-    assert S.level_info(levels - 1, 3)["bf16"] and not S.level_info(levels, 3)["bf16"]
+    assert S.level_info(levels - 1, 3)[half] and not S.level_info(levels, 3)[half]

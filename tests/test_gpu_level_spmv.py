@@ -154,6 +154,50 @@ def test_bf16_cycle_operators_bit_exact(gpu, oracle, nv, tune):
     assert y1.tobytes() == oracle.csr_ax_y(r1, c1.astype(np.uint32), v1, x1, nv).tobytes()
 
 
+def fp16_round(v):
+    """float64 values rounded to float32, divided by the level's power-of-two
+    scale (2^(E-15) for the largest magnitude m * 2^E, m in [0.5, 1)),
+    rounded to FP16 (nearest even) and multiplied back, as float32: what an
+    FP32 level stored in FP16 holds."""
+    f = np.asarray(v, np.float64).astype(np.float32)
+    mx = float(np.abs(f).max())
+    s = np.float32(2.0 ** (np.frexp(mx)[1] - 15)) if mx > 0 else np.float32(1.0)
+    return ((f / s).astype(np.float16).astype(np.float32) * s).astype(np.float32)
+
+
+@pytest.mark.parametrize("nv", [1, 8, 32])
+@pytest.mark.parametrize("tune", [0, 1])
+def test_fp16_cycle_operators_bit_exact(gpu, oracle, nv, tune):
+    """gpu_level_bf16 = 2 with gpu_level_fp16 = 1: the two finest FP32 cycle
+    operators store FP16 values scaled by a per-level power of two and
+    compute in float. Their SpMVs must equal the oracle's float row sums over
+    the values rounded that way bit for bit; the levels below keep float."""
+    row, col, val = gpu.generate_diffusion(27, 14, 13, 12, 1.0, 1.0, 3)
+    params = {"solver": {"method": "MergedPBiCGStab", "rel_tolerance": 1e-8, "max_iters": 5,
+                         "gpu_index_compress": 2},
+              "preconditioner": {"method": "MultiGrid", "mg_max_levels": 3,
+                                 "mg_coarsening_type": 8, "mg_interpolation_type": 6,
+                                 "mg_agg_num_levels": 0, "gpu_spmv_tune": tune,
+                                 "gpu_precond_f32": 1, "gpu_index_compress": 2,
+                                 "gpu_level_bf16": 2, "gpu_level_fp16": 1},
+              "pre_smoother": {"method": "Chebyshev"}, "post_smoother": {"method": "Chebyshev"}}
+    _, _, _, S = solver_on(gpu, row, col, val, nv, params)
+    assert S.level_info(0, 3)["fp16"] and S.level_info(1, 3)["fp16"]
+    assert not S.level_info(0, 3)["bf16"]
+    assert not S.level_info(2, 3)["fp16"]
+    xh, y0, y, ya = run_level_spmv(gpu, S, 0, 3, row, col, val, nv, True, seed=nv)
+    vh = fp16_round(val)
+    assert not np.array_equal(vh, val.astype(np.float32))  # the rounding is real
+    assert y.tobytes() == oracle.csr_ax_y(row, col, vh, xh, nv).tobytes()
+    assert ya.tobytes() == oracle.csr_ax_y(row, col, vh, xh, nv, axpy_y=y0).tobytes()
+    r1, c1, v1, info = S.level_download(1, 3)
+    x1, y01, y1, ya1 = run_level_spmv(gpu, S, 1, 3, r1, c1, v1, nv, True, seed=nv + 1)
+    assert y1.tobytes() == oracle.csr_ax_y(r1, c1.astype(np.uint32), v1, x1, nv).tobytes()
+    # the downloaded level-0 values are the FP16 values times the level's scale
+    _, _, v0, _ = S.level_download(0, 3)
+    assert v0.tobytes() == vh.tobytes()
+
+
 @pytest.mark.parametrize("nv", [1, 2, 8, 32])
 @pytest.mark.parametrize("f32", [False, True])
 def test_warp_per_row_kernel_bit_exact(gpu, oracle, nv, f32):
