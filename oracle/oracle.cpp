@@ -825,8 +825,8 @@ static Csr to_bf16_values(const Csr &a) {
 
 // B200 extension gpu_level_fp16 = 1: the same levels store FP16 values
 // instead, each float value divided by the level's power-of-two scale s
-// (2^(E - 15) for the largest magnitude m * 2^E, m in [0.5, 1); 1 for an
-// all-zero level), rounded to the nearest FP16 (ties to even, IEEE
+// (2^(E - 15) for the largest magnitude m * 2^E, m in [0.5, 1), but at
+// least 2^-126; 1 for an all-zero level), rounded to the nearest FP16 (ties to even, IEEE
 // binary16 through the compiler's _Float16) and read back as h * s; the
 // division and the product by s are exact.
 static Csr to_fp16_values(const Csr &a) {
@@ -837,7 +837,7 @@ static Csr to_fp16_values(const Csr &a) {
     if (mx > 0.0f && std::isfinite(mx)) {
         int E = 0;
         std::frexp(mx, &E);
-        s = std::ldexp(1.0f, E - 15);
+        s = std::ldexp(1.0f, std::max(E - 15, -126));
     }
     for (float &v : b.vf) v = (float)(_Float16)(v / s) * s;
     return b;

@@ -132,7 +132,8 @@ struct DCsr {
     bool f32 = false;
     bool bf16 = false;  // float matrix whose values are stored in BF16
     // float matrix whose values are stored in FP16 divided by vscale, a power
-    // of two that puts the largest magnitude in [2^14, 2^15)
+    // of two that puts the largest magnitude in [2^14, 2^15) (vscale at least
+    // 2^-126)
     bool fp16 = false;
     float vscale = 1.0f;
     uint16_t hash = 0;

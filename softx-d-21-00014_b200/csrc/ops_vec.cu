@@ -519,12 +519,14 @@ void upload_csr(const HCsr &h, DCsr &d, bool f32, int narrow, cudaStream_t s, in
         XG_CUDA(cudaStreamSynchronize(s));
     }
     if (d.fp16) {
-        // scale 2^(E - 15) for the largest magnitude m * 2^E (m in [0.5, 1))
+        // scale 2^(E - 15) for the largest magnitude m * 2^E (m in [0.5, 1)),
+        // at least 2^-126 so that it stays a normal float
         float mx = 0.0f;
         for (double v : h.val) mx = std::max(mx, std::fabs((float)v));
         int E = 0;
         if (mx > 0.0f && std::isfinite(mx)) std::frexp(mx, &E);
-        d.vscale = mx > 0.0f && std::isfinite(mx) ? std::ldexp(1.0f, E - 15) : 1.0f;
+        d.vscale = mx > 0.0f && std::isfinite(mx) ? std::ldexp(1.0f, std::max(E - 15, -126))
+                                                  : 1.0f;
         std::vector<__half> v(h.val.size());
         for (size_t i = 0; i < v.size(); ++i) v[i] = __float2half_rn((float)h.val[i] / d.vscale);
         upload(d.val, v, s);

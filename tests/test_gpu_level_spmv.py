@@ -161,7 +161,7 @@ def fp16_round(v):
     FP32 level stored in FP16 holds."""
     f = np.asarray(v, np.float64).astype(np.float32)
     mx = float(np.abs(f).max())
-    s = np.float32(2.0 ** (np.frexp(mx)[1] - 15)) if mx > 0 else np.float32(1.0)
+    s = np.float32(2.0 ** max(np.frexp(mx)[1] - 15, -126)) if mx > 0 else np.float32(1.0)
     return ((f / s).astype(np.float16).astype(np.float32) * s).astype(np.float32)
 
 
